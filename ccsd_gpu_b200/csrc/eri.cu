@@ -1,0 +1,558 @@
+// Rys-quadrature two-electron integrals and their first derivatives, sm_100a.
+//
+// Replaces fill_int2e_kernel / fill_int2e_ip1_kernel and their launch loops
+// (ref: ccsd_gpu/cuda/int2e_module.py:130-463, ccsd_gpu/cuda/int2e_ip1_module.py:273-667,
+//  ccsd_gpu/cuda/int2e_gpu.py:39-108, ccsd_gpu/cuda/int2e_ip1_gpu.py:148-216).
+//
+// Work decomposition (one warp = one shell quartet, no block-wide barriers):
+//   slot   = (primitive quartet, Rys root); a warp processes its quartet's slots in
+//            batches that fit its shared-memory slice;
+//   phase A  lanes over primitive quartets: Gaussian-product data and the Rys
+//            nodes/weights (each lane evaluates its own roots from the tables);
+//   phase B  lanes over (slot, direction): 2D recurrences + both horizontal
+//            transfers for one Cartesian direction, written to shared memory;
+//   phase C  lanes over output functions: accumulate gx*gy*gz (or the
+//            derivative combination) in registers across all slots.
+// The warp's outputs stay in registers until the quartet is finished, so the
+// output is written once.  Output functions are enumerated with the l-index
+// fastest so neighbouring lanes write neighbouring kl-pair addresses.
+#include "common.cuh"
+#include "rys.cuh"
+
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+namespace cb {
+
+static char g_err[512] = "";
+
+void set_error(const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+}
+
+int check_launch(const char *what)
+{
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error("%s: %s", what, cudaGetErrorString(e));
+        return CCSD_B200_ERR_LAUNCH;
+    }
+    return CCSD_B200_OK;
+}
+
+static constexpr int kWarps = 4;          // warps (quartets in flight) per CTA
+static constexpr int kParStride = 12;     // doubles of per-slot parameters
+static constexpr int kMaxSlots = 64;      // slots per batch cap
+
+// Cartesian exponents, lexicographic order per l (l <= 4), packed x | y<<4 | z<<8
+__constant__ uint16_t c_cart[35] = {
+    0x000,
+    0x001, 0x010, 0x100,
+    0x002, 0x011, 0x101, 0x020, 0x110, 0x200,
+    0x003, 0x012, 0x102, 0x021, 0x111, 0x201, 0x030, 0x120, 0x210, 0x300,
+    0x004, 0x013, 0x103, 0x022, 0x112, 0x202, 0x031, 0x121, 0x211, 0x301,
+    0x040, 0x130, 0x220, 0x310, 0x400};
+__constant__ int c_cart_off[5] = {0, 1, 4, 10, 20};
+
+struct Shell {
+    int l, np;
+    const double *exps, *coefs;
+    double R[3];
+};
+
+__device__ __forceinline__ Shell load_shell(const int *__restrict__ atm, const int *__restrict__ bas,
+                                            const double *__restrict__ env, int sh)
+{
+    Shell s;
+    const int *b = bas + sh * CB_BAS_SLOTS;
+    s.l = b[CB_ANG_OF];
+    s.np = b[CB_NPRIM_OF];
+    s.exps = env + b[CB_PTR_EXP];
+    s.coefs = env + b[CB_PTR_COEFF];
+    const double *r = env + atm[b[CB_ATOM_OF] * CB_ATM_SLOTS + CB_PTR_COORD];
+    s.R[0] = r[0];
+    s.R[1] = r[1];
+    s.R[2] = r[2];
+    return s;
+}
+
+__device__ __forceinline__ double common_fac(int l)
+{
+    return l == 0 ? 0.282094791773878143 : (l == 1 ? 0.488602511902919921 : 1.0);
+}
+
+// One Cartesian direction of one slot: 2D recurrences then HRR on both pairs.
+// Result g[i + j*sj + k*sk + l*sl], i <= li+D, j <= lj, k <= lk, l <= ll.
+template <int D>
+__device__ void build_g(const double *__restrict__ p, int dir, int li, int lj, int lk, int ll,
+                        double ab, double cd, double *__restrict__ g)
+{
+    const int lij = li + lj + D, lkl = lk + ll;
+    const int sj = li + 1 + D, sk = sj * (lj + 1), sl = sk * (lk + 1);
+    const double c00 = p[dir], c01 = p[3 + dir], b00 = p[6], b10 = p[7], b01 = p[8];
+    double t[2 * CB_LMAX + 2][2 * CB_LMAX + 1];   // t[n][m], n <= lij, m <= lkl
+    t[0][0] = dir == 0 ? p[9] : 1.0;
+    if (lij > 0) t[1][0] = c00 * t[0][0];
+    for (int n = 1; n < lij; n++) t[n + 1][0] = c00 * t[n][0] + n * b10 * t[n - 1][0];
+    for (int m = 0; m < lkl; m++) {
+        const double mb = m * b01;
+        t[0][m + 1] = c01 * t[0][m] + (m ? mb * t[0][m - 1] : 0.0);
+        for (int n = 1; n <= lij; n++)
+            t[n][m + 1] = c01 * t[n][m] + (m ? mb * t[n][m - 1] : 0.0) + n * b00 * t[n - 1][m];
+    }
+    // HRR on (i,j): in place, column m at a time; values for j land in g at
+    // i + j*sj + m*sk (fits because sk*(lkl+1) <= sk*(lk+1)*(ll+1)).
+    for (int m = 0; m <= lkl; m++) {
+        double v[2 * CB_LMAX + 2];
+        for (int n = 0; n <= lij; n++) v[n] = t[n][m];
+        for (int i = 0; i <= li + D; i++) g[i + m * sk] = v[i];
+        for (int j = 1; j <= lj; j++) {
+            for (int n = 0; n <= lij - j; n++) v[n] = v[n + 1] + ab * v[n];
+            for (int i = 0; i <= li + D; i++) g[i + j * sj + m * sk] = v[i];
+        }
+    }
+    // HRR on (k,l): per (i,j) column, all writes stay inside the same column
+    if (ll > 0) {
+        for (int o = 0; o < sk; o++) {
+            double w[2 * CB_LMAX + 1];
+            for (int m = 0; m <= lkl; m++) w[m] = g[o + m * sk];
+            for (int l = 1; l <= ll; l++) {
+                for (int m = 0; m <= lkl - l; m++) w[m] = w[m + 1] + cd * w[m];
+                for (int k = 0; k <= lk; k++) g[o + k * sk + l * sl] = w[k];
+            }
+        }
+    }
+}
+
+enum { MODE_S2KL = 0, MODE_QSUM = 1 };
+
+struct S2klOut {
+    double *out;
+    long long nao_pair, comp_stride;
+    int nao, i_base;
+};
+
+// Integrals of one shell quartet by one warp.  MODE_S2KL writes the s2kl block,
+// MODE_QSUM writes two checksums per component of the Cartesian quartet block.
+template <int D, int MODE>
+__device__ void eri_quartet(const int *__restrict__ atm, const int *__restrict__ bas,
+                            const double *__restrict__ env, const int *__restrict__ ao_loc,
+                            int ish, int jsh, int ksh, int lsh, double *__restrict__ wsm, int smem_warp,
+                            const S2klOut &so, double *__restrict__ qsum, int lane)
+{
+    constexpr int NC = D ? 3 : 1;
+    constexpr int GW = D ? 8 : 16;
+    const Shell si = load_shell(atm, bas, env, ish), sj_ = load_shell(atm, bas, env, jsh);
+    const Shell sk_ = load_shell(atm, bas, env, ksh), sl_ = load_shell(atm, bas, env, lsh);
+    const int li = si.l, lj = sj_.l, lk = sk_.l, ll = sl_.l;
+    const int nfi = ncart(li), nfj = ncart(lj), nfk = ncart(lk), nfl = ncart(ll);
+    const int nf = nfi * nfj * nfk * nfl;
+    const int nroots = (li + lj + lk + ll + D) / 2 + 1;
+    const int sj = li + 1 + D, sk = sj * (lj + 1), sl = sk * (lk + 1), gsz = sl * (ll + 1);
+    const int npq = si.np * sj_.np * sk_.np * sl_.np;
+    const int nslot = npq * nroots;
+    int ns = smem_warp / (3 * gsz + kParStride);
+    ns = ns > kMaxSlots ? kMaxSlots : ns;
+    double *par = wsm;
+    double *gbuf = wsm + ns * kParStride;
+    double AB[3], CD[3];
+    for (int x = 0; x < 3; x++) {
+        AB[x] = si.R[x] - sj_.R[x];
+        CD[x] = sk_.R[x] - sl_.R[x];
+    }
+    const double rab2 = AB[0] * AB[0] + AB[1] * AB[1] + AB[2] * AB[2];
+    const double rcd2 = CD[0] * CD[0] + CD[1] * CD[1] + CD[2] * CD[2];
+    const double pref0 = 34.986836655249725693 * common_fac(li) * common_fac(lj) * common_fac(lk) *
+                         common_fac(ll);   // 2 pi^(5/2) x angular factors of s, p
+
+    for (int f0 = 0; f0 < nf; f0 += 32 * GW) {
+        double acc[GW][NC];
+        int gidx[GW];     // ax | ay << 10 | az << 20
+        int iexp[GW];     // ix | iy << 4 | iz << 8 (derivative only)
+#pragma unroll
+        for (int n = 0; n < GW; n++) {
+#pragma unroll
+            for (int c = 0; c < NC; c++) acc[n][c] = 0.0;
+            const int f = f0 + n * 32 + lane;
+            gidx[n] = 0;
+            iexp[n] = 0;
+            if (f < nf) {
+                int t = f;
+                const int fl = t % nfl; t /= nfl;
+                const int fk = t % nfk; t /= nfk;
+                const int fj = t % nfj;
+                const int fi = t / nfj;
+                const int ci = c_cart[c_cart_off[li] + fi], cj = c_cart[c_cart_off[lj] + fj];
+                const int ck = c_cart[c_cart_off[lk] + fk], cl = c_cart[c_cart_off[ll] + fl];
+                const int ax = (ci & 15) + (cj & 15) * sj + (ck & 15) * sk + (cl & 15) * sl;
+                const int ay = ((ci >> 4) & 15) + ((cj >> 4) & 15) * sj + ((ck >> 4) & 15) * sk + ((cl >> 4) & 15) * sl;
+                const int az = (ci >> 8) + (cj >> 8) * sj + (ck >> 8) * sk + (cl >> 8) * sl;
+                gidx[n] = ax | (ay << 10) | (az << 20);
+                iexp[n] = ci;
+            }
+        }
+        for (int s0 = 0; s0 < nslot; s0 += ns) {
+            const int s1 = min(nslot, s0 + ns);
+            __syncwarp();
+            // ---- phase A: primitive-quartet data and Rys nodes/weights
+            const int pq0 = s0 / nroots, pq1 = (s1 - 1) / nroots + 1;
+            for (int pq = pq0 + lane; pq < pq1; pq += 32) {
+                int t = pq;
+                const int lp = t % sl_.np; t /= sl_.np;
+                const int kp = t % sk_.np; t /= sk_.np;
+                const int jp = t % sj_.np;
+                const int ip = t / sj_.np;
+                const double ai = si.exps[ip], aj = sj_.exps[jp], ak = sk_.exps[kp], al = sl_.exps[lp];
+                const double aij = ai + aj, akl = ak + al, aijkl = aij + akl;
+                double PA[3], QC[3], PQ[3];
+                for (int x = 0; x < 3; x++) {
+                    PA[x] = -aj / aij * AB[x];
+                    QC[x] = -al / akl * CD[x];
+                    PQ[x] = (si.R[x] + PA[x]) - (sk_.R[x] + QC[x]);
+                }
+                const double rpq2 = PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2];
+                const double T = aij * akl / aijkl * rpq2;
+                const double pref = pref0 * si.coefs[ip] * sj_.coefs[jp] * sk_.coefs[kp] * sl_.coefs[lp] *
+                                    exp(-ai * aj / aij * rab2 - ak * al / akl * rcd2) / (aij * akl * sqrt(aijkl));
+                double u[RYS_NROOTS_MAX], w[RYS_NROOTS_MAX];
+                rys_roots(nroots, T, u, w);
+                for (int r = 0; r < nroots; r++) {
+                    const int s = pq * nroots + r;
+                    if (s < s0 || s >= s1) continue;
+                    double *p = par + (s - s0) * kParStride;
+                    const double ua = u[r] / aijkl;
+                    for (int x = 0; x < 3; x++) {
+                        p[x] = PA[x] - ua * akl * PQ[x];
+                        p[3 + x] = QC[x] + ua * aij * PQ[x];
+                    }
+                    p[6] = 0.5 * ua;
+                    p[7] = 0.5 / aij * (1.0 - ua * akl);
+                    p[8] = 0.5 / akl * (1.0 - ua * aij);
+                    p[9] = w[r] * pref;
+                    p[10] = 2.0 * ai;
+                }
+            }
+            __syncwarp();
+            // ---- phase B: recurrences, one (slot, direction) per lane
+            for (int it = lane; it < (s1 - s0) * 3; it += 32) {
+                const int s = it / 3, dir = it - s * 3;
+                build_g<D>(par + s * kParStride, dir, li, lj, lk, ll, AB[dir], CD[dir],
+                           gbuf + (s * 3 + dir) * gsz);
+            }
+            __syncwarp();
+            // ---- phase C: accumulate
+            for (int s = 0; s < s1 - s0; s++) {
+                const double *gx = gbuf + s * 3 * gsz, *gy = gx + gsz, *gz = gy + gsz;
+                const double ai2 = par[s * kParStride + 10];
+#pragma unroll
+                for (int n = 0; n < GW; n++) {
+                    if (f0 + n * 32 + lane < nf) {
+                        const int ax = gidx[n] & 1023, ay = (gidx[n] >> 10) & 1023, az = gidx[n] >> 20;
+                        const double x = gx[ax], y = gy[ay], z = gz[az];
+                        if (D == 0) {
+                            acc[n][0] = fma(x * y, z, acc[n][0]);
+                        } else {
+                            const int ix = iexp[n] & 15, iy = (iexp[n] >> 4) & 15, iz = iexp[n] >> 8;
+                            double fx = -ai2 * gx[ax + 1], fy = -ai2 * gy[ay + 1], fz = -ai2 * gz[az + 1];
+                            if (ix) fx = fma((double)ix, gx[ax - 1], fx);
+                            if (iy) fy = fma((double)iy, gy[ay - 1], fy);
+                            if (iz) fz = fma((double)iz, gz[az - 1], fz);
+                            acc[n][0] = fma(fx * y, z, acc[n][0]);
+                            acc[n][NC > 1 ? 1 : 0] = fma(x * fy, z, acc[n][NC > 1 ? 1 : 0]);
+                            acc[n][NC > 2 ? 2 : 0] = fma(x * y, fz, acc[n][NC > 2 ? 2 : 0]);
+                        }
+                    }
+                }
+            }
+        }
+        // ---- epilogue
+        if (MODE == MODE_S2KL) {
+            const int i0 = ao_loc[ish] - so.i_base, j0 = ao_loc[jsh], k0 = ao_loc[ksh], l0 = ao_loc[lsh];
+#pragma unroll
+            for (int n = 0; n < GW; n++) {
+                const int f = f0 + n * 32 + lane;
+                if (f < nf) {
+                    int t = f;
+                    const int fl = t % nfl; t /= nfl;
+                    const int fk = t % nfk; t /= nfk;
+                    const int fj = t % nfj;
+                    const int fi = t / nfj;
+                    if (ksh == lsh && fl > fk) continue;
+                    const long long k = k0 + fk, l = l0 + fl;
+                    const long long addr = ((long long)(i0 + fi) * so.nao + (j0 + fj)) * so.nao_pair + k * (k + 1) / 2 + l;
+#pragma unroll
+                    for (int c = 0; c < NC; c++) so.out[c * so.comp_stride + addr] = acc[n][c];
+                }
+            }
+        } else {
+#pragma unroll
+            for (int c = 0; c < NC; c++) {
+                double s1v = 0.0, s2v = 0.0;
+#pragma unroll
+                for (int n = 0; n < GW; n++) {
+                    const int f = f0 + n * 32 + lane;
+                    if (f < nf) {
+                        s1v += acc[n][c] * (1.0 + 0.125 * (f & 7));
+                        s2v += acc[n][c] * acc[n][c];
+                    }
+                }
+                for (int o = 16; o > 0; o >>= 1) {
+                    s1v += __shfl_xor_sync(0xffffffffu, s1v, o);
+                    s2v += __shfl_xor_sync(0xffffffffu, s2v, o);
+                }
+                if (lane == 0) {
+                    qsum[2 * c] += s1v;
+                    qsum[2 * c + 1] += s2v;
+                }
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void decode_pair(long long p, int &k, int &l)
+{
+    int kk = (int)((sqrt(8.0 * (double)p + 1.0) - 1.0) * 0.5);
+    while ((long long)kk * (kk + 1) / 2 > p) kk--;
+    while ((long long)(kk + 1) * (kk + 2) / 2 <= p) kk++;
+    k = kk;
+    l = (int)(p - (long long)kk * (kk + 1) / 2);
+}
+
+// s2kl block of shells [ish0, ish1) x all j x all k >= l (decontracted shells).
+template <int D>
+__global__ void __launch_bounds__(kWarps * 32) eri_s2kl_kernel(
+    const int *__restrict__ atm, const int *__restrict__ bas, const double *__restrict__ env,
+    const int *__restrict__ ao_loc, int ish0, int ish1, int nbas, int nao, double *__restrict__ out,
+    int smem_warp)
+{
+    extern __shared__ double smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double *wsm = smem + warp * smem_warp;
+    const long long npairs = (long long)nbas * (nbas + 1) / 2;
+    const long long nq = (long long)(ish1 - ish0) * nbas * npairs;
+    S2klOut so;
+    so.out = out;
+    so.nao = nao;
+    so.nao_pair = (long long)nao * (nao + 1) / 2;
+    so.comp_stride = (long long)(ao_loc[ish1] - ao_loc[ish0]) * nao * so.nao_pair;
+    so.i_base = ao_loc[ish0];
+    for (long long q = (long long)blockIdx.x * kWarps + warp; q < nq; q += (long long)gridDim.x * kWarps) {
+        const long long ij = q / npairs;
+        int ksh, lsh;
+        decode_pair(q - ij * npairs, ksh, lsh);
+        const int ish = ish0 + (int)(ij / nbas), jsh = (int)(ij % nbas);
+        eri_quartet<D, MODE_S2KL>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, wsm, smem_warp, so, nullptr, lane);
+    }
+}
+
+// Explicit quartet list (int4 shells), two checksums per component per quartet.
+template <int D>
+__global__ void __launch_bounds__(kWarps * 32) eri_qsum_kernel(
+    const int *__restrict__ atm, const int *__restrict__ bas, const double *__restrict__ env,
+    const int4 *__restrict__ quartets, long long nq, double *__restrict__ qsum, int smem_warp)
+{
+    extern __shared__ double smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double *wsm = smem + warp * smem_warp;
+    S2klOut so = {};
+    constexpr int NC = D ? 3 : 1;
+    for (long long q = (long long)blockIdx.x * kWarps + warp; q < nq; q += (long long)gridDim.x * kWarps) {
+        const int4 s = quartets[q];
+        double acc[2 * NC];
+        for (int c = 0; c < 2 * NC; c++) acc[c] = 0.0;
+        eri_quartet<D, MODE_QSUM>(atm, bas, env, nullptr, s.x, s.y, s.z, s.w, wsm, smem_warp, so, acc, lane);
+        if (lane == 0)
+            for (int c = 0; c < 2 * NC; c++) qsum[q * 2 * NC + c] = acc[c];
+    }
+}
+
+// ---- Cartesian -> spherical transform of an s2kl block (two passes) ----
+// Sparse block-diagonal cart2sph: spherical AO s has coefficients
+// val[ptr[s]..ptr[s+1]) on Cartesian AOs idx[...].
+
+// pass 1: (ncomp, nfc, naoc, npc) -> (ncomp, nfs, naos, npc), transforms i and j
+__global__ void c2s_ij_kernel(const double *__restrict__ in, double *__restrict__ out, int ncomp,
+                              int nfc, int naoc, long long npc, int nfs, int naos,
+                              const int *__restrict__ ptr_i, const int *__restrict__ idx_i,
+                              const double *__restrict__ val_i, const int *__restrict__ ptr,
+                              const int *__restrict__ idx, const double *__restrict__ val)
+{
+    const long long total = (long long)ncomp * nfs * naos * npc;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const long long kl = e % npc;
+        long long t = e / npc;
+        const int js = (int)(t % naos);
+        t /= naos;
+        const int is = (int)(t % nfs);
+        const int c = (int)(t / nfs);
+        double acc = 0.0;
+        for (int a = ptr_i[is]; a < ptr_i[is + 1]; a++)
+            for (int b = ptr[js]; b < ptr[js + 1]; b++)
+                acc += val_i[a] * val[b] * in[(((long long)c * nfc + idx_i[a]) * naoc + idx[b]) * npc + kl];
+        out[e] = acc;
+    }
+}
+
+// pass 2: (rows, npc) -> (rows, nps), transforms k and l with s2 symmetry
+__global__ void c2s_kl_kernel(const double *__restrict__ in, double *__restrict__ out, long long rows,
+                              long long npc, int naos, const int *__restrict__ ptr,
+                              const int *__restrict__ idx, const double *__restrict__ val)
+{
+    const long long nps = (long long)naos * (naos + 1) / 2;
+    const long long total = rows * nps;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const long long r = e / nps, p = e - r * nps;
+        int ks, ls;
+        decode_pair(p, ks, ls);
+        const double *row = in + r * npc;
+        double acc = 0.0;
+        for (int a = ptr[ks]; a < ptr[ks + 1]; a++)
+            for (int b = ptr[ls]; b < ptr[ls + 1]; b++) {
+                const long long kc = idx[a], lc = idx[b];
+                const long long pc = kc >= lc ? kc * (kc + 1) / 2 + lc : lc * (lc + 1) / 2 + kc;
+                acc += val[a] * val[b] * row[pc];
+            }
+        out[e] = acc;
+    }
+}
+
+static int smem_per_warp(int lmax, int deriv)
+{
+    const int gsz = (lmax + 1 + deriv) * (lmax + 1) * (lmax + 1) * (lmax + 1);
+    int need = 3 * gsz + kParStride;
+    return need < 2048 ? 2048 : need;
+}
+
+static int num_sms()
+{
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 148;
+    }
+    return n;
+}
+
+template <typename K>
+static int prepare_kernel(K kernel, size_t smem)
+{
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) {
+            set_error("cudaFuncSetAttribute: %s", cudaGetErrorString(e));
+            return CCSD_B200_ERR_LAUNCH;
+        }
+    }
+    return CCSD_B200_OK;
+}
+
+}  // namespace cb
+
+using namespace cb;
+
+extern "C" {
+
+const char *ccsd_b200_last_error(void) { return g_err; }
+
+int ccsd_b200_eri_s2kl_cart(int deriv, const int32_t *atm, const int32_t *bas, const double *env, int nbas,
+                            const int32_t *ao_loc, int ish0, int ish1, int nao, int lmax, double *out,
+                            void *stream)
+{
+    if (deriv < 0 || deriv > 1 || !atm || !bas || !env || !ao_loc || !out || nbas <= 0 || ish0 < 0 ||
+        ish1 > nbas || ish0 >= ish1 || nao <= 0 || lmax < 0) {
+        set_error("ccsd_b200_eri_s2kl_cart: invalid argument");
+        return CCSD_B200_ERR_ARG;
+    }
+    if (lmax > CB_LMAX) {
+        set_error("ccsd_b200_eri_s2kl_cart: l = %d > %d is not supported", lmax, CB_LMAX);
+        return CCSD_B200_ERR_UNSUPPORTED;
+    }
+    const int sw = smem_per_warp(lmax, deriv);
+    const size_t smem = (size_t)sw * kWarps * sizeof(double);
+    const long long nq = (long long)(ish1 - ish0) * nbas * ((long long)nbas * (nbas + 1) / 2);
+    long long grid = (nq + kWarps - 1) / kWarps;
+    const long long gmax = (long long)num_sms() * 16;
+    if (grid > gmax) grid = gmax;
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc;
+    if (deriv) {
+        if ((rc = prepare_kernel(eri_s2kl_kernel<1>, smem))) return rc;
+        eri_s2kl_kernel<1><<<(int)grid, kWarps * 32, smem, st>>>(atm, bas, env, ao_loc, ish0, ish1, nbas, nao,
+                                                                  out, sw);
+    } else {
+        if ((rc = prepare_kernel(eri_s2kl_kernel<0>, smem))) return rc;
+        eri_s2kl_kernel<0><<<(int)grid, kWarps * 32, smem, st>>>(atm, bas, env, ao_loc, ish0, ish1, nbas, nao,
+                                                                  out, sw);
+    }
+    return check_launch("eri_s2kl_kernel");
+}
+
+int ccsd_b200_eri_quartet_checksums(int deriv, const int32_t *atm, const int32_t *bas, const double *env,
+                                    const int32_t *quartets, long long nq, int lmax, double *qsum,
+                                    void *stream)
+{
+    if (deriv < 0 || deriv > 1 || !atm || !bas || !env || !quartets || !qsum || nq < 0 || lmax < 0) {
+        set_error("ccsd_b200_eri_quartet_checksums: invalid argument");
+        return CCSD_B200_ERR_ARG;
+    }
+    if (lmax > CB_LMAX) {
+        set_error("ccsd_b200_eri_quartet_checksums: l = %d > %d is not supported", lmax, CB_LMAX);
+        return CCSD_B200_ERR_UNSUPPORTED;
+    }
+    if (nq == 0) return CCSD_B200_OK;
+    const int sw = smem_per_warp(lmax, deriv);
+    const size_t smem = (size_t)sw * kWarps * sizeof(double);
+    long long grid = (nq + kWarps - 1) / kWarps;
+    const long long gmax = (long long)num_sms() * 16;
+    if (grid > gmax) grid = gmax;
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc;
+    const int4 *q4 = reinterpret_cast<const int4 *>(quartets);
+    if (deriv) {
+        if ((rc = prepare_kernel(eri_qsum_kernel<1>, smem))) return rc;
+        eri_qsum_kernel<1><<<(int)grid, kWarps * 32, smem, st>>>(atm, bas, env, q4, nq, qsum, sw);
+    } else {
+        if ((rc = prepare_kernel(eri_qsum_kernel<0>, smem))) return rc;
+        eri_qsum_kernel<0><<<(int)grid, kWarps * 32, smem, st>>>(atm, bas, env, q4, nq, qsum, sw);
+    }
+    return check_launch("eri_qsum_kernel");
+}
+
+int ccsd_b200_cart2sph_s2kl(const double *cart, double *tmp, double *out, int ncomp, int nfc, int naoc, int nfs,
+                            int naos, const int32_t *ptr_i, const int32_t *idx_i, const double *val_i,
+                            const int32_t *ptr, const int32_t *idx, const double *val, void *stream)
+{
+    if (!cart || !tmp || !out || ncomp <= 0 || nfc <= 0 || naoc <= 0 || nfs <= 0 || naos <= 0 || !ptr_i ||
+        !idx_i || !val_i || !ptr || !idx || !val) {
+        set_error("ccsd_b200_cart2sph_s2kl: invalid argument");
+        return CCSD_B200_ERR_ARG;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    const long long npc = (long long)naoc * (naoc + 1) / 2;
+    const long long rows = (long long)ncomp * nfs * naos;
+    const long long t1 = rows * npc;
+    const int bs = 256;
+    long long g1 = (t1 + bs - 1) / bs;
+    const long long gmax = (long long)num_sms() * 32;
+    if (g1 > gmax) g1 = gmax;
+    c2s_ij_kernel<<<(int)g1, bs, 0, st>>>(cart, tmp, ncomp, nfc, naoc, npc, nfs, naos, ptr_i, idx_i, val_i, ptr,
+                                          idx, val);
+    int rc = check_launch("c2s_ij_kernel");
+    if (rc) return rc;
+    const long long t2 = rows * ((long long)naos * (naos + 1) / 2);
+    long long g2 = (t2 + bs - 1) / bs;
+    if (g2 > gmax) g2 = gmax;
+    c2s_kl_kernel<<<(int)g2, bs, 0, st>>>(tmp, out, rows, npc, naos, ptr, idx, val);
+    return check_launch("c2s_kl_kernel");
+}
+
+}  // extern "C"

@@ -1,0 +1,141 @@
+"""Seeded synthetic inputs for the benchmarks and the full-size parity checks.
+
+ERI microbenchmark shells: 4096 shells, l in {0, 1, 2} with probabilities
+4/9, 3/9, 2/9, 1..6 primitives each, exponents log-uniform in [0.05, 1e4],
+contraction coefficients uniform in [0.1, 1] then normalised with the PySCF
+convention, centres uniform in a 12-bohr cube, every shell on its own centre.
+"""
+import numpy as np
+
+from .gto.mole import BAS_SLOTS, PTR_ENV_START, normalized_coefficients
+
+
+class ShellSet:
+    """_atm/_bas/_env of a synthetic set of (decontracted) shells."""
+
+    def __init__(self, atm, bas, env):
+        self._atm = np.ascontiguousarray(atm, dtype=np.int32)
+        self._bas = np.ascontiguousarray(bas, dtype=np.int32)
+        self._env = np.ascontiguousarray(env, dtype=np.float64)
+
+    @property
+    def nbas(self):
+        return len(self._bas)
+
+    @property
+    def lmax(self):
+        return int(self._bas[:, 1].max())
+
+
+def eri_bench_shells(nshell=4096, seed=0, lvals=(0, 1, 2), lprob=(4 / 9, 3 / 9, 2 / 9), max_prim=6,
+                     box=12.0, exp_range=(0.05, 1e4)):
+    rng = np.random.default_rng(seed)
+    env = [0.0] * PTR_ENV_START
+    atm, bas = [], []
+    ls = rng.choice(np.asarray(lvals), size=nshell, p=np.asarray(lprob))
+    for ish in range(nshell):
+        xyz = rng.uniform(0.0, box, 3)
+        ptr = len(env)
+        env.extend(xyz.tolist())
+        env.append(0.0)
+        atm.append([1, ptr, 1, ptr + 3, 0, 0])
+        l = int(ls[ish])
+        nprim = int(rng.integers(1, max_prim + 1))
+        es = np.sort(10.0 ** rng.uniform(np.log10(exp_range[0]), np.log10(exp_range[1]), nprim))[::-1]
+        cs = rng.uniform(0.1, 1.0, nprim)
+        cs = normalized_coefficients(l, es, cs[:, None])[:, 0]
+        pe = len(env)
+        env.extend(es.tolist())
+        pc = len(env)
+        env.extend(cs.tolist())
+        bas.append([ish, l, nprim, 1, 0, pe, pc, 0])
+    return ShellSet(np.array(atm).reshape(-1, 6), np.array(bas).reshape(-1, BAS_SLOTS), np.array(env))
+
+
+def lclass(bas, q):
+    """Unique L-class id of quartets q (n, 4): sorted (li>=lj), (lk>=ll), pair order."""
+    l = bas[:, 1][q]
+    a = np.maximum(l[:, 0], l[:, 1]) * 10 + np.minimum(l[:, 0], l[:, 1])
+    b = np.maximum(l[:, 2], l[:, 3]) * 10 + np.minimum(l[:, 2], l[:, 3])
+    return np.maximum(a, b) * 100 + np.minimum(a, b)
+
+
+def sample_quartets(shells, n, seed=1, schwarz_fn=None, threshold=1e-12, oversample=4):
+    """Uniform sample of unique quartets (i>=j, k>=l, ij>=kl) passing the screen.
+
+    schwarz_fn(pairs) -> Q for an (m, 2) array of shell pairs.  Quartets are
+    returned sorted by L-class (the kernels process them class-batched).
+    """
+    rng = np.random.default_rng(seed)
+    nb = shells.nbas
+    out = []
+    have = 0
+    while have < n:
+        m = (n - have) * oversample + 1024
+        i = rng.integers(0, nb, m)
+        j = rng.integers(0, nb, m)
+        k = rng.integers(0, nb, m)
+        l = rng.integers(0, nb, m)
+        ij = np.stack([np.maximum(i, j), np.minimum(i, j)], 1)
+        kl = np.stack([np.maximum(k, l), np.minimum(k, l)], 1)
+        pij = ij[:, 0].astype(np.int64) * (ij[:, 0] + 1) // 2 + ij[:, 1]
+        pkl = kl[:, 0].astype(np.int64) * (kl[:, 0] + 1) // 2 + kl[:, 1]
+        swap = pkl > pij
+        a = np.where(swap[:, None], kl, ij)
+        b = np.where(swap[:, None], ij, kl)
+        q = np.concatenate([a, b], 1).astype(np.int32)
+        if schwarz_fn is not None:
+            pairs = np.concatenate([q[:, :2], q[:, 2:]], 0)
+            keys = pairs[:, 0].astype(np.int64) * nb + pairs[:, 1]
+            uk, inv = np.unique(keys, return_inverse=True)
+            vals = np.asarray(schwarz_fn(np.stack([uk // nb, uk % nb], 1).astype(np.int32)))
+            qv = vals[inv]
+            keep = qv[:m] * qv[m:] > threshold
+            q = q[keep]
+        out.append(q)
+        have += len(q)
+    q = np.concatenate(out, 0)[:n]
+    order = np.argsort(lclass(shells._bas, q), kind="stable")
+    return np.ascontiguousarray(q[order])
+
+
+def ncart(l):
+    return (l + 1) * (l + 2) // 2
+
+
+def reference_flops(li, lj, lk, ll, npi, npj, npk, npl, deriv):
+    """FP64 operation count of the reference algorithm for one shell quartet.
+
+    Counted from the loop structure of fill_int2e_kernel / fill_int2e_ip1_kernel
+    (ref: ccsd_gpu/cuda/int2e_module.py:253-430, ccsd_gpu/cuda/int2e_ip1_module.py:401-629),
+    per primitive quartet: 29 for the Gaussian-product setup (:263-279), the
+    Rys evaluation 2n (2*13 + 4) (ref: int2e_ip1_module.py:222-243), and per
+    root 10 for the recurrence coefficients (:287-294), the vertical, transfer
+    and two horizontal recurrences, and the accumulation (3 per output for
+    int2e, 21 per output triple for int2e_ip1, ref: int2e_ip1_module.py:620-629).
+    """
+    nroots = (li + lj + lk + ll + deriv) // 2 + 1
+    lij = li + lj + deriv
+    lkl = lk + ll
+    nf = ncart(li) * ncart(lj) * ncart(lk) * ncart(ll)
+    sj = li + 1 + deriv
+    sk = sj * (lj + 1)
+    vrr = 3 * (1 + 4 * max(lij - 1, 0)) if lij > 0 else 0
+    trr = 3 * (lij + 1) * lkl * 6
+    hrr_ij = 3 * (lkl + 1) * sum(2 * (lij - j + 1) for j in range(lj))
+    hrr_kl = 3 * sk * sum(2 * (lkl - l + 1) for l in range(ll))
+    acc = (21 if deriv else 3) * nf
+    per_root = 10 + vrr + trr + hrr_ij + hrr_kl + acc
+    per_prim = 29 + 2 * nroots * (2 * 13 + 4) + nroots * per_root
+    return per_prim * npi * npj * npk * npl
+
+
+def quartet_flops(shells, q, deriv):
+    b = shells._bas
+    l = b[:, 1][q]
+    npr = b[:, 2][q]
+    total = 0
+    keys, counts = np.unique(np.concatenate([l, npr], 1), axis=0, return_counts=True)
+    for key, c in zip(keys, counts):
+        total += int(c) * reference_flops(*[int(v) for v in key], deriv)
+    return total

@@ -1,0 +1,90 @@
+/*
+ * ccsd_b200.h -- C ABI of libccsdb200.so (B200 / sm_100a CCSD gradient hot path).
+ *
+ * Conventions for every entry point:
+ *   - all array arguments are DEVICE pointers owned by the caller;
+ *   - work is enqueued on `stream` (a cudaStream_t, NULL = legacy default stream)
+ *     and the call returns without synchronising;
+ *   - the return value is a status: 0 = CCSD_B200_OK, otherwise one of the
+ *     CCSD_B200_ERR_* codes, with a message from ccsd_b200_last_error();
+ *   - nothing throws across the ABI; the library is not thread-safe for
+ *     concurrent calls from several host threads.
+ * Shell data use the libcint/PySCF layout: atm rows of 6 int32
+ * [Z, ptr_coord, ...], bas rows of 8 int32 [atom, l, nprim, nctr, kappa,
+ * ptr_exp, ptr_coeff, 0], env float64.  ERI entry points take DECONTRACTED
+ * shells (nctr == 1; split general contractions first) and l <= 4.
+ */
+#ifndef CCSD_B200_H
+#define CCSD_B200_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CCSD_B200_OK 0
+#define CCSD_B200_ERR_ARG 1
+#define CCSD_B200_ERR_LAUNCH 2
+#define CCSD_B200_ERR_TIMEOUT 3
+#define CCSD_B200_ERR_NONFINITE 4
+#define CCSD_B200_ERR_UNSUPPORTED 5
+
+/* Message of the last failing call (static storage). */
+const char *ccsd_b200_last_error(void);
+
+/*
+ * Cartesian s2kl block of (ij|kl) (deriv = 0) or d/dr_1 (ij|kl) (deriv = 1)
+ * for i-shells [ish0, ish1), all j-shells and all k >= l shell pairs:
+ *   out[comp][i - ao_loc[ish0]][j][k*(k+1)/2 + l],  k >= l,
+ * comp = x, y, z for deriv = 1.  Every element of the block is written.
+ * ao_loc: Cartesian AO offsets of the nbas decontracted shells (nbas + 1
+ * entries); nao = ao_loc[nbas]; lmax = max l over the shells.
+ * Replaces fill_int2e_kernel / fill_int2e_ip1_kernel and the per-i-shell
+ * launch loop of _compute_cart
+ * (ref: ccsd_gpu/cuda/int2e_module.py:130-463, ccsd_gpu/cuda/int2e_gpu.py:39-108,
+ *       ccsd_gpu/cuda/int2e_ip1_module.py:273-667, ccsd_gpu/cuda/int2e_ip1_gpu.py:148-216).
+ */
+int ccsd_b200_eri_s2kl_cart(int deriv, const int32_t *atm, const int32_t *bas, const double *env,
+                            int nbas, const int32_t *ao_loc, int ish0, int ish1, int nao, int lmax,
+                            double *out, void *stream);
+
+/*
+ * Integrals of an explicit list of shell quartets (int32 x 4 per quartet,
+ * [i, j, k, l]), consumed in-kernel: per quartet and component two checksums
+ *   qsum[q][comp][0] = sum_f v_f * (1 + (f mod 8)/8),  qsum[q][comp][1] = sum_f v_f^2
+ * over the Cartesian functions f = ((fi*nfj + fj)*nfk + fk)*nfl + fl.
+ * Used by the ERI throughput benchmark and its parity checks; no counterpart
+ * in the reference (which only stores full blocks, ref: ccsd_gpu/cuda/int2e_gpu.py:81-106).
+ */
+int ccsd_b200_eri_quartet_checksums(int deriv, const int32_t *atm, const int32_t *bas, const double *env,
+                                    const int32_t *quartets, long long nq, int lmax, double *qsum,
+                                    void *stream);
+
+/*
+ * Cartesian -> spherical transform of an s2kl block:
+ * cart (ncomp, nfc, naoc, naoc(naoc+1)/2) -> out (ncomp, nfs, naos, naos(naos+1)/2),
+ * tmp (ncomp, nfs, naos, naoc(naoc+1)/2) is caller-provided scratch.  The
+ * transform matrix is given by columns in CSR form: spherical function s of
+ * the i-block has coefficients val_i[ptr_i[s]..ptr_i[s+1]) on Cartesian rows
+ * idx_i[...] of the block; (ptr, idx, val) is the same for the whole basis.
+ * Replaces _cart_to_sph_eri0 / _cart_to_sph_eri1, which unpack to a dense
+ * nao_cart^2 square (ref: ccsd_gpu/cuda/int2e_gpu.py:115-179,
+ * ccsd_gpu/cuda/int2e_ip1_gpu.py:223-289).
+ */
+int ccsd_b200_cart2sph_s2kl(const double *cart, double *tmp, double *out, int ncomp, int nfc, int naoc,
+                            int nfs, int naos, const int32_t *ptr_i, const int32_t *idx_i,
+                            const double *val_i, const int32_t *ptr, const int32_t *idx,
+                            const double *val, void *stream);
+
+/*
+ * FP64 FMA throughput probe: `blocks` x 256 threads, each running 8
+ * independent FMA chains for `iters` iterations (2*8*iters*256*blocks FLOPs).
+ * `out` needs blocks*256 doubles (written only in a practically unreachable
+ * branch).  Used to measure the FP64 roofline of the ERI kernels; no
+ * counterpart in the reference.
+ */
+int ccsd_b200_fp64_fma_probe(double *out, int blocks, int iters, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -48,6 +48,8 @@ def lib():
         _lib.oracle_eri_s2kl.argtypes = [_i32p, ctypes.c_int, _i32p, ctypes.c_int, _f64p,
                                          _i32p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _f64p]
         _lib.oracle_eri_quartet.argtypes = [_i32p, _i32p, _f64p] + [ctypes.c_int] * 5 + [_f64p]
+        _lib.oracle_eri_quartet_checksums.argtypes = [ctypes.c_int, _i32p, _i32p, _f64p, _i32p,
+                                                      ctypes.c_long, _f64p]
     return _lib
 
 
@@ -63,6 +65,8 @@ def ref():
                                       ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                       _i32p, ctypes.c_int]
         _ref.ref_rys_roots.argtypes = [ctypes.c_int, ctypes.c_double, _f64p, _f64p]
+        _ref.ref_eri_quartet_checksums.argtypes = [ctypes.c_int, _i32p, _i32p, _f64p, _i32p,
+                                                   ctypes.c_long, _f64p]
     return _ref
 
 
@@ -164,3 +168,14 @@ def s2kl(mol, b0, b1, deriv=0, impl="oracle"):
     if not mol.cart:
         cart = cart_to_sph(cart, mol, b0, b1)
     return cart if deriv else cart[0]
+
+
+def quartet_checksums(shells, quartets, deriv, impl="oracle"):
+    """(nq, ncomp, 2) checksums of explicit quartets on the CPU (all OpenMP threads)."""
+    atm, bas, env = _arrays(shells)
+    q = np.ascontiguousarray(quartets, dtype=np.int32).reshape(-1, 4)
+    ncomp = 3 if deriv else 1
+    out = np.zeros(len(q) * ncomp * 2)
+    fn = lib().oracle_eri_quartet_checksums if impl == "oracle" else ref().ref_eri_quartet_checksums
+    fn(int(deriv), atm, bas, env, q.ravel(), len(q), out)
+    return out.reshape(len(q), ncomp, 2)

@@ -188,6 +188,14 @@ void oracle_rys_roots(int n, double x, double *u_out, double *w_out)
 /* Boys function F_m(x), m = 0..mmax, by series + downward recursion (for tests). */
 void oracle_boys(int mmax, double x, double *F)
 {
+    if (x > 300.0) {   /* exp(-x) below long-double resolution: F_m = (2m-1)/(2x) F_{m-1} */
+        long double Fm = sqrtl(3.14159265358979323846264338327950288L / (4.0L * x));
+        for (int m = 0; m <= mmax; m++) {
+            F[m] = (double)Fm;
+            Fm *= (2 * m + 1) / (2.0L * x);
+        }
+        return;
+    }
     long double lx = x, ex = expl(-lx), term = 1.0L / (2 * mmax + 1), s = term;
     for (int k = 1; k < 200000; k++) {
         term *= 2 * lx / (2 * mmax + 2 * k + 1);
@@ -436,5 +444,43 @@ int oracle_eri_quartet(const int *atm, const int *bas, const double *env,
     load_shell(bas, env, atm, ksh, &q.lk, &q.npk, &q.nck, &q.ak, &q.ck, &q.C);
     load_shell(bas, env, atm, lsh, &q.ll, &q.npl, &q.ncl, &q.al, &q.cl, &q.D);
     shell_quartet(&q, deriv, out);
+    return 0;
+}
+
+int oracle_eri_quartet(const int *atm, const int *bas, const double *env,
+                       int ish, int jsh, int ksh, int lsh, int deriv, double *out);
+
+/* Two checksums per quartet and component, same definition as
+ * ccsd_b200_eri_quartet_checksums; decontracted shells only. */
+int oracle_eri_quartet_checksums(int deriv, const int *atm, const int *bas, const double *env,
+                                 const int *quartets, long nq, double *qsum)
+{
+    const int ncomp = deriv ? 3 : 1;
+    gl_init();
+#pragma omp parallel for schedule(dynamic, 16)
+    for (long q = 0; q < nq; q++) {
+        const int *s = quartets + 4 * q;
+        int nf = 1;
+        for (int t = 0; t < 4; t++) nf *= ncart(bas[s[t] * BAS_SLOTS + ANG_OF]);
+        double *buf = (double *)malloc(sizeof(double) * nf * ncomp);
+        oracle_eri_quartet(atm, bas, env, s[0], s[1], s[2], s[3], deriv, buf);
+        const int nfi = ncart(bas[s[0] * BAS_SLOTS + ANG_OF]), nfj = ncart(bas[s[1] * BAS_SLOTS + ANG_OF]);
+        const int nfk = ncart(bas[s[2] * BAS_SLOTS + ANG_OF]), nfl = ncart(bas[s[3] * BAS_SLOTS + ANG_OF]);
+        for (int c = 0; c < ncomp; c++) {
+            double s1 = 0, s2 = 0;
+            int f = 0;
+            for (int fi = 0; fi < nfi; fi++)
+                for (int fj = 0; fj < nfj; fj++)
+                    for (int fk = 0; fk < nfk; fk++)
+                        for (int fl = 0; fl < nfl; fl++, f++) {
+                            const double v = buf[c * nf + ((fl * nfk + fk) * nfj + fj) * nfi + fi];
+                            s1 += v * (1.0 + 0.125 * (f & 7));
+                            s2 += v * v;
+                        }
+            qsum[(q * ncomp + c) * 2] = s1;
+            qsum[(q * ncomp + c) * 2 + 1] = s2;
+        }
+        free(buf);
+    }
     return 0;
 }
