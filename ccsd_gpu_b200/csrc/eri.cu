@@ -129,6 +129,87 @@ __device__ void build_g(const double *__restrict__ p, int dir, int li, int lj, i
     }
 }
 
+// Same recurrences as build_g with compile-time angular momenta (l <= 2),
+// streamed: the transfer recurrence keeps two columns (m-1, m) of the 2D table
+// in registers, each finished column goes through the (i,j) horizontal
+// recurrence straight into shared memory, and the (k,l) horizontal recurrence
+// runs per (i,j) column from there.  Peak live state is ~4 (LIJ+1) doubles.
+template <int D, int LI, int LJ, int LK, int LL>
+__device__ __forceinline__ void build_g_fixed(const double *__restrict__ p, int dir, double ab, double cd,
+                                              double *__restrict__ g)
+{
+    constexpr int LIJ = LI + LJ + D, LKL = LK + LL;
+    constexpr int SJ = LI + 1 + D, SK = SJ * (LJ + 1), SL = SK * (LK + 1);
+    const double c00 = p[dir], c01 = p[3 + dir], b00 = p[6], b10 = p[7], b01 = p[8];
+    double prev[LIJ + 1], cur[LIJ + 1];
+    cur[0] = dir == 0 ? p[9] : 1.0;
+#pragma unroll
+    for (int n = 0; n < LIJ; n++) cur[n + 1] = c00 * cur[n] + (n ? n * b10 * cur[n - 1] : 0.0);
+#pragma unroll
+    for (int n = 0; n <= LIJ; n++) prev[n] = 0.0;
+#pragma unroll
+    for (int m = 0; m <= LKL; m++) {
+        {   // HRR (i,j) of column m into g[i + j*SJ + m*SK]
+            double v[LIJ + 1];
+#pragma unroll
+            for (int n = 0; n <= LIJ; n++) v[n] = cur[n];
+#pragma unroll
+            for (int i = 0; i <= LI + D; i++) g[i + m * SK] = v[i];
+#pragma unroll
+            for (int j = 1; j <= LJ; j++) {
+#pragma unroll
+                for (int n = 0; n <= LIJ - j; n++) v[n] = v[n + 1] + ab * v[n];
+#pragma unroll
+                for (int i = 0; i <= LI + D; i++) g[i + j * SJ + m * SK] = v[i];
+            }
+        }
+        if (m < LKL) {
+            double nxt[LIJ + 1];
+#pragma unroll
+            for (int n = 0; n <= LIJ; n++)
+                nxt[n] = c01 * cur[n] + (m ? m * b01 * prev[n] : 0.0) + (n ? n * b00 * cur[n - 1] : 0.0);
+#pragma unroll
+            for (int n = 0; n <= LIJ; n++) {
+                prev[n] = cur[n];
+                cur[n] = nxt[n];
+            }
+        }
+    }
+    if (LL > 0) {
+#pragma unroll
+        for (int o = 0; o < SK; o++) {
+            double w[LKL + 1];
+#pragma unroll
+            for (int m = 0; m <= LKL; m++) w[m] = g[o + m * SK];
+#pragma unroll
+            for (int l = 1; l <= LL; l++) {
+#pragma unroll
+                for (int m = 0; m <= LKL - l; m++) w[m] = w[m + 1] + cd * w[m];
+#pragma unroll
+                for (int k = 0; k <= LK; k++) g[o + k * SK + l * SL] = w[k];
+            }
+        }
+    }
+}
+
+#define CB_G(c) case c: build_g_fixed<D, (c) / 27, ((c) / 9) % 3, ((c) / 3) % 3, (c) % 3>(p, dir, ab, cd, g); return;
+#define CB_G9(b) CB_G(b) CB_G(b + 1) CB_G(b + 2) CB_G(b + 3) CB_G(b + 4) CB_G(b + 5) CB_G(b + 6) CB_G(b + 7) CB_G(b + 8)
+
+template <int D, bool LOW>
+__device__ __forceinline__ void build_g_any(const double *__restrict__ p, int dir, int li, int lj, int lk, int ll,
+                                            double ab, double cd, double *__restrict__ g)
+{
+    if (LOW || (li <= 2 && lj <= 2 && lk <= 2 && ll <= 2)) {
+        switch (li * 27 + lj * 9 + lk * 3 + ll) {
+            CB_G9(0) CB_G9(9) CB_G9(18) CB_G9(27) CB_G9(36) CB_G9(45) CB_G9(54) CB_G9(63) CB_G9(72)
+            default: break;
+        }
+    }
+    if (!LOW) build_g<D>(p, dir, li, lj, lk, ll, ab, cd, g);
+}
+#undef CB_G9
+#undef CB_G
+
 enum { MODE_S2KL = 0, MODE_QSUM = 1 };
 
 struct S2klOut {
@@ -139,14 +220,14 @@ struct S2klOut {
 
 // Integrals of one shell quartet by one warp.  MODE_S2KL writes the s2kl block,
 // MODE_QSUM writes two checksums per component of the Cartesian quartet block.
-template <int D, int MODE>
+template <int D, int MODE, bool LOW>
 __device__ void eri_quartet(const int *__restrict__ atm, const int *__restrict__ bas,
                             const double *__restrict__ env, const int *__restrict__ ao_loc,
                             int ish, int jsh, int ksh, int lsh, double *__restrict__ wsm, int smem_warp,
                             const S2klOut &so, double *__restrict__ qsum, int lane)
 {
     constexpr int NC = D ? 3 : 1;
-    constexpr int GW = D ? 8 : 16;
+    constexpr int GW = 8;
     const Shell si = load_shell(atm, bas, env, ish), sj_ = load_shell(atm, bas, env, jsh);
     const Shell sk_ = load_shell(atm, bas, env, ksh), sl_ = load_shell(atm, bas, env, lsh);
     const int li = si.l, lj = sj_.l, lk = sk_.l, ll = sl_.l;
@@ -170,17 +251,23 @@ __device__ void eri_quartet(const int *__restrict__ atm, const int *__restrict__
     const double pref0 = 34.986836655249725693 * common_fac(li) * common_fac(lj) * common_fac(lk) *
                          common_fac(ll);   // 2 pi^(5/2) x angular factors of s, p
 
-    for (int f0 = 0; f0 < nf; f0 += 32 * GW) {
+    // Small blocks: the warp splits into NG slot groups of FW lanes (FW >= nf),
+    // each group accumulates a strided subset of the slots, and the groups are
+    // reduced with shuffles at the end.  nf >= 32: one group, GW outputs per lane.
+    const int FW = nf >= 32 ? 32 : (nf > 16 ? 32 : (nf > 8 ? 16 : (nf > 4 ? 8 : (nf > 2 ? 4 : (nf > 1 ? 2 : 1)))));
+    const int NG = 32 / FW;
+    const int flane = lane & (FW - 1), grp = lane / FW;
+    for (int f0 = 0; f0 < nf; f0 += FW * GW) {
         double acc[GW][NC];
         int gidx[GW];     // ax | ay << 10 | az << 20
-        int iexp[GW];     // ix | iy << 4 | iz << 8 (derivative only)
+        int iexp[D ? GW : 1];     // ix | iy << 4 | iz << 8 (derivative only)
 #pragma unroll
         for (int n = 0; n < GW; n++) {
 #pragma unroll
             for (int c = 0; c < NC; c++) acc[n][c] = 0.0;
-            const int f = f0 + n * 32 + lane;
+            const int f = f0 + n * FW + flane;
             gidx[n] = 0;
-            iexp[n] = 0;
+            if (D) iexp[D ? n : 0] = 0;
             if (f < nf) {
                 int t = f;
                 const int fl = t % nfl; t /= nfl;
@@ -193,7 +280,7 @@ __device__ void eri_quartet(const int *__restrict__ atm, const int *__restrict__
                 const int ay = ((ci >> 4) & 15) + ((cj >> 4) & 15) * sj + ((ck >> 4) & 15) * sk + ((cl >> 4) & 15) * sl;
                 const int az = (ci >> 8) + (cj >> 8) * sj + (ck >> 8) * sk + (cl >> 8) * sl;
                 gidx[n] = ax | (ay << 10) | (az << 20);
-                iexp[n] = ci;
+                if (D) iexp[D ? n : 0] = ci;
             }
         }
         for (int s0 = 0; s0 < nslot; s0 += ns) {
@@ -241,23 +328,24 @@ __device__ void eri_quartet(const int *__restrict__ atm, const int *__restrict__
             // ---- phase B: recurrences, one (slot, direction) per lane
             for (int it = lane; it < (s1 - s0) * 3; it += 32) {
                 const int s = it / 3, dir = it - s * 3;
-                build_g<D>(par + s * kParStride, dir, li, lj, lk, ll, AB[dir], CD[dir],
-                           gbuf + (s * 3 + dir) * gsz);
+                build_g_any<D, LOW>(par + s * kParStride, dir, li, lj, lk, ll, AB[dir], CD[dir],
+                               gbuf + (s * 3 + dir) * gsz);
             }
             __syncwarp();
             // ---- phase C: accumulate
-            for (int s = 0; s < s1 - s0; s++) {
+            for (int s = grp; s < s1 - s0; s += NG) {
                 const double *gx = gbuf + s * 3 * gsz, *gy = gx + gsz, *gz = gy + gsz;
                 const double ai2 = par[s * kParStride + 10];
 #pragma unroll
                 for (int n = 0; n < GW; n++) {
-                    if (f0 + n * 32 + lane < nf) {
+                    if (f0 + n * FW + flane < nf) {
                         const int ax = gidx[n] & 1023, ay = (gidx[n] >> 10) & 1023, az = gidx[n] >> 20;
                         const double x = gx[ax], y = gy[ay], z = gz[az];
                         if (D == 0) {
                             acc[n][0] = fma(x * y, z, acc[n][0]);
                         } else {
-                            const int ix = iexp[n] & 15, iy = (iexp[n] >> 4) & 15, iz = iexp[n] >> 8;
+                            const int ie = iexp[D ? n : 0];
+                            const int ix = ie & 15, iy = (ie >> 4) & 15, iz = ie >> 8;
                             double fx = -ai2 * gx[ax + 1], fy = -ai2 * gy[ay + 1], fz = -ai2 * gz[az + 1];
                             if (ix) fx = fma((double)ix, gx[ax - 1], fx);
                             if (iy) fy = fma((double)iy, gy[ay - 1], fy);
@@ -270,13 +358,21 @@ __device__ void eri_quartet(const int *__restrict__ atm, const int *__restrict__
                 }
             }
         }
+        // ---- reduce the slot groups
+        if (NG > 1) {
+#pragma unroll
+            for (int n = 0; n < GW; n++)
+#pragma unroll
+                for (int c = 0; c < NC; c++)
+                    for (int o = FW; o < 32; o <<= 1) acc[n][c] += __shfl_xor_sync(0xffffffffu, acc[n][c], o);
+        }
         // ---- epilogue
         if (MODE == MODE_S2KL) {
             const int i0 = ao_loc[ish] - so.i_base, j0 = ao_loc[jsh], k0 = ao_loc[ksh], l0 = ao_loc[lsh];
 #pragma unroll
             for (int n = 0; n < GW; n++) {
-                const int f = f0 + n * 32 + lane;
-                if (f < nf) {
+                const int f = f0 + n * FW + flane;
+                if (f < nf && grp == 0) {
                     int t = f;
                     const int fl = t % nfl; t /= nfl;
                     const int fk = t % nfk; t /= nfk;
@@ -295,8 +391,8 @@ __device__ void eri_quartet(const int *__restrict__ atm, const int *__restrict__
                 double s1v = 0.0, s2v = 0.0;
 #pragma unroll
                 for (int n = 0; n < GW; n++) {
-                    const int f = f0 + n * 32 + lane;
-                    if (f < nf) {
+                    const int f = f0 + n * FW + flane;
+                    if (f < nf && grp == 0) {
                         s1v += acc[n][c] * (1.0 + 0.125 * (f & 7));
                         s2v += acc[n][c] * acc[n][c];
                     }
@@ -324,8 +420,8 @@ __device__ __forceinline__ void decode_pair(long long p, int &k, int &l)
 }
 
 // s2kl block of shells [ish0, ish1) x all j x all k >= l (decontracted shells).
-template <int D>
-__global__ void __launch_bounds__(kWarps * 32) eri_s2kl_kernel(
+template <int D, bool LOW>
+__global__ void __launch_bounds__(kWarps * 32, LOW ? (D ? 2 : 3) : 2) eri_s2kl_kernel(
     const int *__restrict__ atm, const int *__restrict__ bas, const double *__restrict__ env,
     const int *__restrict__ ao_loc, int ish0, int ish1, int nbas, int nao, double *__restrict__ out,
     int smem_warp)
@@ -346,13 +442,13 @@ __global__ void __launch_bounds__(kWarps * 32) eri_s2kl_kernel(
         int ksh, lsh;
         decode_pair(q - ij * npairs, ksh, lsh);
         const int ish = ish0 + (int)(ij / nbas), jsh = (int)(ij % nbas);
-        eri_quartet<D, MODE_S2KL>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, wsm, smem_warp, so, nullptr, lane);
+        eri_quartet<D, MODE_S2KL, LOW>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, wsm, smem_warp, so, nullptr, lane);
     }
 }
 
 // Explicit quartet list (int4 shells), two checksums per component per quartet.
-template <int D>
-__global__ void __launch_bounds__(kWarps * 32) eri_qsum_kernel(
+template <int D, bool LOW>
+__global__ void __launch_bounds__(kWarps * 32, LOW ? (D ? 2 : 3) : 2) eri_qsum_kernel(
     const int *__restrict__ atm, const int *__restrict__ bas, const double *__restrict__ env,
     const int4 *__restrict__ quartets, long long nq, double *__restrict__ qsum, int smem_warp)
 {
@@ -365,7 +461,7 @@ __global__ void __launch_bounds__(kWarps * 32) eri_qsum_kernel(
         const int4 s = quartets[q];
         double acc[2 * NC];
         for (int c = 0; c < 2 * NC; c++) acc[c] = 0.0;
-        eri_quartet<D, MODE_QSUM>(atm, bas, env, nullptr, s.x, s.y, s.z, s.w, wsm, smem_warp, so, acc, lane);
+        eri_quartet<D, MODE_QSUM, LOW>(atm, bas, env, nullptr, s.x, s.y, s.z, s.w, wsm, smem_warp, so, acc, lane);
         if (lane == 0)
             for (int c = 0; c < 2 * NC; c++) qsum[q * 2 * NC + c] = acc[c];
     }
@@ -484,15 +580,16 @@ int ccsd_b200_eri_s2kl_cart(int deriv, const int32_t *atm, const int32_t *bas, c
     if (grid > gmax) grid = gmax;
     cudaStream_t st = (cudaStream_t)stream;
     int rc;
+#define CB_LAUNCH_S2KL(DV, LOWV)                                                                              \
+    if ((rc = prepare_kernel(eri_s2kl_kernel<DV, LOWV>, smem))) return rc;                                     \
+    eri_s2kl_kernel<DV, LOWV><<<(int)grid, kWarps * 32, smem, st>>>(atm, bas, env, ao_loc, ish0, ish1, nbas, nao, \
+                                                                     out, sw);
     if (deriv) {
-        if ((rc = prepare_kernel(eri_s2kl_kernel<1>, smem))) return rc;
-        eri_s2kl_kernel<1><<<(int)grid, kWarps * 32, smem, st>>>(atm, bas, env, ao_loc, ish0, ish1, nbas, nao,
-                                                                  out, sw);
+        if (lmax <= 2) { CB_LAUNCH_S2KL(1, true) } else { CB_LAUNCH_S2KL(1, false) }
     } else {
-        if ((rc = prepare_kernel(eri_s2kl_kernel<0>, smem))) return rc;
-        eri_s2kl_kernel<0><<<(int)grid, kWarps * 32, smem, st>>>(atm, bas, env, ao_loc, ish0, ish1, nbas, nao,
-                                                                  out, sw);
+        if (lmax <= 2) { CB_LAUNCH_S2KL(0, true) } else { CB_LAUNCH_S2KL(0, false) }
     }
+#undef CB_LAUNCH_S2KL
     return check_launch("eri_s2kl_kernel");
 }
 
@@ -517,13 +614,15 @@ int ccsd_b200_eri_quartet_checksums(int deriv, const int32_t *atm, const int32_t
     cudaStream_t st = (cudaStream_t)stream;
     int rc;
     const int4 *q4 = reinterpret_cast<const int4 *>(quartets);
+#define CB_LAUNCH_QSUM(DV, LOWV)                                                       \
+    if ((rc = prepare_kernel(eri_qsum_kernel<DV, LOWV>, smem))) return rc;              \
+    eri_qsum_kernel<DV, LOWV><<<(int)grid, kWarps * 32, smem, st>>>(atm, bas, env, q4, nq, qsum, sw);
     if (deriv) {
-        if ((rc = prepare_kernel(eri_qsum_kernel<1>, smem))) return rc;
-        eri_qsum_kernel<1><<<(int)grid, kWarps * 32, smem, st>>>(atm, bas, env, q4, nq, qsum, sw);
+        if (lmax <= 2) { CB_LAUNCH_QSUM(1, true) } else { CB_LAUNCH_QSUM(1, false) }
     } else {
-        if ((rc = prepare_kernel(eri_qsum_kernel<0>, smem))) return rc;
-        eri_qsum_kernel<0><<<(int)grid, kWarps * 32, smem, st>>>(atm, bas, env, q4, nq, qsum, sw);
+        if (lmax <= 2) { CB_LAUNCH_QSUM(0, true) } else { CB_LAUNCH_QSUM(0, false) }
     }
+#undef CB_LAUNCH_QSUM
     return check_launch("eri_qsum_kernel");
 }
 
