@@ -20,11 +20,15 @@ _vp = ctypes.c_void_p
 SIGNATURES = {
     "ccsd_b200_last_error": (ctypes.c_char_p, []),
     "ccsd_b200_eri_s2kl_cart": (_c_int, [_c_int, _vp, _vp, _vp, _c_int, _vp, _c_int, _c_int, _c_int,
-                                         _c_int, _vp, _vp]),
+                                         _c_int, _vp, _c_ll, _vp, _vp]),
     "ccsd_b200_eri_quartet_checksums": (_c_int, [_c_int, _vp, _vp, _vp, _vp, _c_ll, _c_int, _vp, _vp]),
     "ccsd_b200_cart2sph_s2kl": (_c_int, [_vp, _vp, _vp, _c_int, _c_int, _c_int, _c_int, _c_int,
                                          _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "ccsd_b200_fp64_fma_probe": (_c_int, [_vp, _c_int, _c_int, _vp]),
+    "ccsd_b200_split_pack": (_c_int, [_c_int, _vp, _vp, _vp, _c_dbl, _vp, _vp, _vp, _c_dbl, _c_int, _c_int,
+                                      _c_int, _c_int, _vp, _vp, _vp]),
+    "ccsd_b200_tc_split_gemm": (_c_int, [_c_int, _vp, _vp, _vp, _vp, _c_int, _c_int, _c_int, _c_int, _c_int,
+                                         _vp, _vp, _vp, _c_dbl, _c_dbl, _vp, _vp]),
 }
 
 

@@ -49,6 +49,7 @@ def build(force=False, verbose=False, ptxas_info=False):
     os.makedirs(BUILD_DIR, exist_ok=True)
     objs = []
     hdrs = headers()
+    cmds = []
     for src in sources():
         obj = os.path.join(BUILD_DIR, os.path.basename(src) + ".o")
         objs.append(obj)
@@ -59,7 +60,12 @@ def build(force=False, verbose=False, ptxas_info=False):
                 cmd += ["-Xptxas", "-v"]
             if verbose:
                 print(" ".join(cmd), flush=True)
-            subprocess.check_call(cmd)
+            cmds.append(cmd)
+    # translation units compile in parallel
+    procs = [subprocess.Popen(c) for c in cmds]
+    failed = [c for p, c in zip(procs, cmds) if p.wait() != 0]
+    if failed:
+        raise subprocess.CalledProcessError(1, failed[0])
     if force or _stale(LIB, objs):
         cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
         if verbose:

@@ -1,0 +1,184 @@
+"""Tensor contractions for the Lambda / density-matrix path.
+
+``contract(spec, a, b, out=..., alpha=1, beta=0, mode=...)`` evaluates one
+two-operand einsum ``spec`` (e.g. ``"jabd,jkcd->abkc"``) as a GEMM
+D[m, n] = sum_k A[m, k] B[n, k]:
+
+  * M = indices of ``a`` that survive, N = indices of ``b`` that survive, K = the
+    summed indices; M and N are ordered as in the output string.  An index
+    present in all three is a batch index and is looped on the host.
+  * mode "tf32x3" / "bf16x3": the operands are gathered through element-offset
+    tables, split into hi + lo parts and packed for TMA by one kernel
+    (``ccsd_b200_split_pack``), multiplied on the tcgen05 tensor cores
+    (``ccsd_b200_tc_split_gemm``: hi*hi + hi*lo + lo*hi, FP32 accumulation in
+    512-k chunks drained to FP64), and the result is scattered straight into
+    ``out`` with alpha/beta -- no permuted copy of any operand or of the result
+    is materialised.  An operand may be a linear combination of two views
+    (``[(2.0, t2), (-1.0, t2p)]``), which fuses the ``2 t - t^T`` patterns of
+    the CCSD equations into the pack.
+  * mode "fp64": ``torch.einsum`` in float64 (cuBLAS DGEMM): the plain FP64 GPU
+    path the split-precision modes are measured against.
+"""
+import numpy as np
+import torch
+
+from . import _native
+
+KIND = {"tf32x3": 0, "bf16x3": 1}
+MODES = ("fp64", "tf32x3", "bf16x3")
+_BM = 128
+_KALIGN = {"tf32x3": 32, "bf16x3": 64}
+
+
+def _parse(spec):
+    lhs, out = spec.replace(" ", "").split("->")
+    a, b = lhs.split(",")
+    return a, b, out
+
+
+def _terms(x):
+    if isinstance(x, torch.Tensor):
+        return [(1.0, x)]
+    return [(float(c), t) for c, t in x]
+
+
+def _offsets(idx_order, sub, shape_map, tensor):
+    """Element offsets over the row-major grid of idx_order for a tensor indexed by `sub`."""
+    if not idx_order:
+        return np.zeros(1, dtype=np.int64)
+    st = dict(zip(sub, tensor.stride()))
+    off = np.zeros(1, dtype=np.int64)
+    for ix in idx_order:
+        n = shape_map[ix]
+        off = (off[:, None] + np.arange(n, dtype=np.int64)[None, :] * st.get(ix, 0)).ravel()
+    return off
+
+
+class _Status:
+    buf = {}
+
+    @classmethod
+    def get(cls, dev):
+        t = cls.buf.get(dev)
+        if t is None:
+            t = torch.zeros(1, dtype=torch.int32, device=dev)
+            cls.buf[dev] = t
+        return t
+
+
+def check_status(device=None):
+    """Raise if any tensor-core GEMM since the last check recorded an expired wait."""
+    dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+    st = _Status.get(dev)
+    v = int(st.item())
+    if v:
+        st.zero_()
+        raise _native.NativeError("tensor-core GEMM pipeline wait expired (code %d)" % v)
+
+
+_off_cache = {}
+
+
+def _dev_offsets(key, make, dev):
+    t = _off_cache.get((key, dev))
+    if t is None:
+        t = torch.from_numpy(np.ascontiguousarray(make())).to(dev)
+        if len(_off_cache) > 4096:
+            _off_cache.clear()
+        _off_cache[(key, dev)] = t
+    return t
+
+
+def _pack(terms, sub, rows_idx, k_idx, shape_map, kind, rows_pad, k_pad, dev, stream):
+    rows = int(np.prod([shape_map[i] for i in rows_idx])) if rows_idx else 1
+    K = int(np.prod([shape_map[i] for i in k_idx])) if k_idx else 1
+    esz = 4 if kind == 0 else 2
+    hi = torch.empty(rows_pad * k_pad * esz, dtype=torch.uint8, device=dev)
+    lo = torch.empty_like(hi)
+    offs = []
+    for _, t in terms[:2]:
+        key_r = ("r", tuple(rows_idx), sub, tuple(t.stride()), tuple(shape_map[i] for i in rows_idx))
+        key_k = ("k", tuple(k_idx), sub, tuple(t.stride()), tuple(shape_map[i] for i in k_idx))
+        offs.append((_dev_offsets(key_r, lambda t=t: _offsets(rows_idx, sub, shape_map, t), dev),
+                     _dev_offsets(key_k, lambda t=t: _offsets(k_idx, sub, shape_map, t), dev)))
+    (c1, t1), (o1r, o1k) = terms[0], offs[0]
+    if len(terms) > 1:
+        (c2, t2), (o2r, o2k) = terms[1], offs[1]
+        p2 = (_native.ptr(t2), _native.ptr(o2r), _native.ptr(o2k), c2)
+    else:
+        p2 = (_native.ptr(None), _native.ptr(None), _native.ptr(None), 0.0)
+    _native.call("ccsd_b200_split_pack", kind, _native.ptr(t1), _native.ptr(o1r), _native.ptr(o1k), c1, *p2,
+                 rows, K, rows_pad, k_pad, _native.ptr(hi), _native.ptr(lo), stream)
+    return hi, lo
+
+
+def contract(spec, a, b, out=None, alpha=1.0, beta=0.0, mode="tf32x3", stream=None):
+    """out[...] = alpha * einsum(spec, a, b) + beta * out  (returns out)."""
+    ta, tb = _terms(a), _terms(b)
+    if len(ta) > 2 or len(tb) > 2:
+        raise ValueError("an operand may have at most two terms")
+    sa, sb, so = _parse(spec)
+    shape_map = {}
+    for sub, terms in ((sa, ta), (sb, tb)):
+        for _, t in terms:
+            if t.dim() != len(sub):
+                raise ValueError("operand rank does not match %r" % spec)
+            for ix, n in zip(sub, t.shape):
+                if shape_map.setdefault(ix, n) != n:
+                    raise ValueError("size mismatch for index %r in %r" % (ix, spec))
+    dev = ta[0][1].device
+    if out is None:
+        out = torch.zeros([shape_map[i] for i in so], dtype=torch.float64, device=dev)
+        beta = 0.0
+    if mode == "fp64":
+        res = None
+        for c1, t1 in ta:
+            for c2, t2 in tb:
+                r = torch.einsum(spec, t1, t2) * (c1 * c2)
+                res = r if res is None else res + r
+        if beta == 0.0:
+            out.copy_(res * alpha)
+        else:
+            out.mul_(beta).add_(res, alpha=alpha)
+        return out
+    if mode not in KIND:
+        raise ValueError("unknown mode %r" % mode)
+    _native.require_cuda(out)
+    batch = [i for i in so if i in sa and i in sb]
+    if batch:
+        ix = batch[0]
+        for v in range(shape_map[ix]):
+            sel = lambda sub, t: t.select(sub.index(ix), v)   # noqa: E731
+            a_v = [(c, sel(sa, t)) for c, t in ta]
+            b_v = [(c, sel(sb, t)) for c, t in tb]
+            spec_v = "%s,%s->%s" % (sa.replace(ix, ""), sb.replace(ix, ""), so.replace(ix, ""))
+            contract(spec_v, a_v, b_v, out=out.select(so.index(ix), v), alpha=alpha, beta=beta, mode=mode,
+                     stream=stream)
+        return out
+    m_idx = [i for i in so if i in sa]
+    n_idx = [i for i in so if i in sb]
+    k_idx = [i for i in sa if i in sb and i not in so]
+    for i in sa + sb:
+        if i not in so and not (i in sa and i in sb):
+            raise ValueError("index %r summed in one operand only: not a GEMM" % i)
+    M = int(np.prod([shape_map[i] for i in m_idx])) if m_idx else 1
+    N = int(np.prod([shape_map[i] for i in n_idx])) if n_idx else 1
+    K = int(np.prod([shape_map[i] for i in k_idx])) if k_idx else 1
+    if M == 0 or N == 0:
+        return out
+    kind = KIND[mode]
+    kal = _KALIGN[mode]
+    m_pad = -(-M // _BM) * _BM
+    n_pad = -(-N // _BM) * _BM
+    k_pad = max(kal, -(-K // kal) * kal)
+    st = _native.stream(stream)
+    ahi, alo = _pack(ta, sa, m_idx, k_idx, shape_map, kind, m_pad, k_pad, dev, st)
+    bhi, blo = _pack(tb, sb, n_idx, k_idx, shape_map, kind, n_pad, k_pad, dev, st)
+    key_m = ("om", tuple(m_idx), so, tuple(out.stride()), tuple(shape_map[i] for i in m_idx))
+    key_n = ("on", tuple(n_idx), so, tuple(out.stride()), tuple(shape_map[i] for i in n_idx))
+    om = _dev_offsets(key_m, lambda: _offsets(m_idx, so, shape_map, out), dev)
+    on = _dev_offsets(key_n, lambda: _offsets(n_idx, so, shape_map, out), dev)
+    _native.call("ccsd_b200_tc_split_gemm", kind, _native.ptr(ahi), _native.ptr(alo), _native.ptr(bhi),
+                 _native.ptr(blo), M, N, m_pad, n_pad, k_pad, _native.ptr(out), _native.ptr(om), _native.ptr(on),
+                 float(alpha), float(beta), _native.ptr(_Status.get(dev)), st)
+    return out

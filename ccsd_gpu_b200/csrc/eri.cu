@@ -135,7 +135,7 @@ __device__ void build_g(const double *__restrict__ p, int dir, int li, int lj, i
 // recurrence straight into shared memory, and the (k,l) horizontal recurrence
 // runs per (i,j) column from there.  Peak live state is ~4 (LIJ+1) doubles.
 template <int D, int LI, int LJ, int LK, int LL>
-__device__ __forceinline__ void build_g_fixed(const double *__restrict__ p, int dir, double ab, double cd,
+__device__ __noinline__ void build_g_fixed(const double *__restrict__ p, int dir, double ab, double cd,
                                               double *__restrict__ g)
 {
     constexpr int LIJ = LI + LJ + D, LKL = LK + LL;
@@ -410,6 +410,201 @@ __device__ void eri_quartet(const int *__restrict__ atm, const int *__restrict__
     }
 }
 
+// Quartets whose Cartesian block has more functions than this go to the
+// CTA-cooperative kernel; smaller ones are one warp each.
+static constexpr int kHeavyNf = 1000;
+
+__device__ __forceinline__ int quartet_nf(const int *__restrict__ bas, int i, int j, int k, int l)
+{
+    return ncart(bas[i * CB_BAS_SLOTS + CB_ANG_OF]) * ncart(bas[j * CB_BAS_SLOTS + CB_ANG_OF]) *
+           ncart(bas[k * CB_BAS_SLOTS + CB_ANG_OF]) * ncart(bas[l * CB_BAS_SLOTS + CB_ANG_OF]);
+}
+
+// One heavy shell quartet per CTA (256 threads).  Same three phases as the
+// warp kernel, with the CTA's threads sharing one slot batch (up to 64 slots)
+// and the (output, component) entries spread 16 per thread in registers, so
+// blocks of up to 4096 entries never recompute the recurrences; larger (l > 2)
+// blocks are done in chunks of 4096 entries.
+static constexpr int kHeavyThreads = 256;
+static constexpr int kHeavyAcc = 16;
+
+template <int D, int MODE, bool LOW>
+__device__ void eri_quartet_cta(const int *__restrict__ atm, const int *__restrict__ bas,
+                                const double *__restrict__ env, const int *__restrict__ ao_loc, int ish, int jsh,
+                                int ksh, int lsh, double *__restrict__ sm, int smem_doubles, const S2klOut &so,
+                                double *__restrict__ qsum)
+{
+    constexpr int NC = D ? 3 : 1;
+    const int tid = threadIdx.x;
+    const Shell si = load_shell(atm, bas, env, ish), sj_ = load_shell(atm, bas, env, jsh);
+    const Shell sk_ = load_shell(atm, bas, env, ksh), sl_ = load_shell(atm, bas, env, lsh);
+    const int li = si.l, lj = sj_.l, lk = sk_.l, ll = sl_.l;
+    const int nfi = ncart(li), nfj = ncart(lj), nfk = ncart(lk), nfl = ncart(ll);
+    const int nf = nfi * nfj * nfk * nfl;
+    const int ne = nf * NC;
+    const int nroots = (li + lj + lk + ll + D) / 2 + 1;
+    const int sj = li + 1 + D, sk = sj * (lj + 1), sl = sk * (lk + 1), gsz = sl * (ll + 1);
+    const int nslot = si.np * sj_.np * sk_.np * sl_.np * nroots;
+    int ns = smem_doubles / (3 * gsz + kParStride);
+    ns = ns > kMaxSlots ? kMaxSlots : ns;
+    double *par = sm;
+    double *gbuf = sm + ns * kParStride;
+    double AB[3], CD[3];
+    for (int x = 0; x < 3; x++) {
+        AB[x] = si.R[x] - sj_.R[x];
+        CD[x] = sk_.R[x] - sl_.R[x];
+    }
+    const double rab2 = AB[0] * AB[0] + AB[1] * AB[1] + AB[2] * AB[2];
+    const double rcd2 = CD[0] * CD[0] + CD[1] * CD[1] + CD[2] * CD[2];
+    const double pref0 = 34.986836655249725693 * common_fac(li) * common_fac(lj) * common_fac(lk) * common_fac(ll);
+    double qv[6] = {0, 0, 0, 0, 0, 0};
+
+    for (int e0 = 0; e0 < ne; e0 += kHeavyThreads * kHeavyAcc) {
+        double acc[kHeavyAcc];
+        int gidx[kHeavyAcc];      // ax | ay << 10 | az << 20
+        int ginfo[kHeavyAcc];     // component | ix << 2 | iy << 6 | iz << 10
+#pragma unroll
+        for (int n = 0; n < kHeavyAcc; n++) {
+            acc[n] = 0.0;
+            gidx[n] = 0;
+            ginfo[n] = 0;
+            const int e = e0 + tid + n * kHeavyThreads;
+            if (e < ne) {
+                const int f = e / NC, c = e - f * NC;
+                int t = f;
+                const int fl = t % nfl; t /= nfl;
+                const int fk = t % nfk; t /= nfk;
+                const int fj = t % nfj;
+                const int fi = t / nfj;
+                const int ci = c_cart[c_cart_off[li] + fi], cj = c_cart[c_cart_off[lj] + fj];
+                const int ck = c_cart[c_cart_off[lk] + fk], cl = c_cart[c_cart_off[ll] + fl];
+                const int ax = (ci & 15) + (cj & 15) * sj + (ck & 15) * sk + (cl & 15) * sl;
+                const int ay = ((ci >> 4) & 15) + ((cj >> 4) & 15) * sj + ((ck >> 4) & 15) * sk + ((cl >> 4) & 15) * sl;
+                const int az = (ci >> 8) + (cj >> 8) * sj + (ck >> 8) * sk + (cl >> 8) * sl;
+                gidx[n] = ax | (ay << 10) | (az << 20);
+                ginfo[n] = c | ((ci & 15) << 2) | (((ci >> 4) & 15) << 6) | ((ci >> 8) << 10);
+            }
+        }
+        for (int s0 = 0; s0 < nslot; s0 += ns) {
+            const int s1 = min(nslot, s0 + ns);
+            __syncthreads();
+            const int pq0 = s0 / nroots, pq1 = (s1 - 1) / nroots + 1;
+            for (int pq = pq0 + tid; pq < pq1; pq += kHeavyThreads) {
+                int t = pq;
+                const int lp = t % sl_.np; t /= sl_.np;
+                const int kp = t % sk_.np; t /= sk_.np;
+                const int jp = t % sj_.np;
+                const int ip = t / sj_.np;
+                const double ai = si.exps[ip], aj = sj_.exps[jp], ak = sk_.exps[kp], al = sl_.exps[lp];
+                const double aij = ai + aj, akl = ak + al, aijkl = aij + akl;
+                double PA[3], QC[3], PQ[3];
+                for (int x = 0; x < 3; x++) {
+                    PA[x] = -aj / aij * AB[x];
+                    QC[x] = -al / akl * CD[x];
+                    PQ[x] = (si.R[x] + PA[x]) - (sk_.R[x] + QC[x]);
+                }
+                const double rpq2 = PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2];
+                const double T = aij * akl / aijkl * rpq2;
+                const double pref = pref0 * si.coefs[ip] * sj_.coefs[jp] * sk_.coefs[kp] * sl_.coefs[lp] *
+                                    exp(-ai * aj / aij * rab2 - ak * al / akl * rcd2) / (aij * akl * sqrt(aijkl));
+                double u[RYS_NROOTS_MAX], w[RYS_NROOTS_MAX];
+                rys_roots(nroots, T, u, w);
+                for (int r = 0; r < nroots; r++) {
+                    const int s = pq * nroots + r;
+                    if (s < s0 || s >= s1) continue;
+                    double *p = par + (s - s0) * kParStride;
+                    const double ua = u[r] / aijkl;
+                    for (int x = 0; x < 3; x++) {
+                        p[x] = PA[x] - ua * akl * PQ[x];
+                        p[3 + x] = QC[x] + ua * aij * PQ[x];
+                    }
+                    p[6] = 0.5 * ua;
+                    p[7] = 0.5 / aij * (1.0 - ua * akl);
+                    p[8] = 0.5 / akl * (1.0 - ua * aij);
+                    p[9] = w[r] * pref;
+                    p[10] = 2.0 * ai;
+                }
+            }
+            __syncthreads();
+            for (int it = tid; it < (s1 - s0) * 3; it += kHeavyThreads) {
+                const int s = it / 3, dir = it - s * 3;
+                build_g_any<D, LOW>(par + s * kParStride, dir, li, lj, lk, ll, AB[dir], CD[dir],
+                                    gbuf + (s * 3 + dir) * gsz);
+            }
+            __syncthreads();
+            for (int s = 0; s < s1 - s0; s++) {
+                const double *gx = gbuf + s * 3 * gsz, *gy = gx + gsz, *gz = gy + gsz;
+                const double ai2 = par[s * kParStride + 10];
+#pragma unroll
+                for (int n = 0; n < kHeavyAcc; n++) {
+                    if (e0 + tid + n * kHeavyThreads < ne) {
+                        const int ax = gidx[n] & 1023, ay = (gidx[n] >> 10) & 1023, az = gidx[n] >> 20;
+                        if (D == 0) {
+                            acc[n] = fma(gx[ax] * gy[ay], gz[az], acc[n]);
+                        } else {
+                            const int c = ginfo[n] & 3;
+                            const int ie = c == 0 ? (ginfo[n] >> 2) & 15 : (c == 1 ? (ginfo[n] >> 6) & 15 : ginfo[n] >> 10);
+                            const double *gd = c == 0 ? gx : (c == 1 ? gy : gz);
+                            const int ad = c == 0 ? ax : (c == 1 ? ay : az);
+                            double fd = -ai2 * gd[ad + 1];
+                            if (ie) fd = fma((double)ie, gd[ad - 1], fd);
+                            const double px = c == 0 ? fd : gx[ax];
+                            const double py = c == 1 ? fd : gy[ay];
+                            const double pz = c == 2 ? fd : gz[az];
+                            acc[n] = fma(px * py, pz, acc[n]);
+                        }
+                    }
+                }
+            }
+        }
+        // ---- epilogue of this chunk
+        if (MODE == MODE_S2KL) {
+            const int i0 = ao_loc[ish] - so.i_base, j0 = ao_loc[jsh], k0 = ao_loc[ksh], l0 = ao_loc[lsh];
+#pragma unroll
+            for (int n = 0; n < kHeavyAcc; n++) {
+                const int e = e0 + tid + n * kHeavyThreads;
+                if (e < ne) {
+                    const int f = e / NC, c = e - f * NC;
+                    int t = f;
+                    const int fl = t % nfl; t /= nfl;
+                    const int fk = t % nfk; t /= nfk;
+                    const int fj = t % nfj;
+                    const int fi = t / nfj;
+                    if (ksh == lsh && fl > fk) continue;
+                    const long long k = k0 + fk, l = l0 + fl;
+                    so.out[c * so.comp_stride + ((long long)(i0 + fi) * so.nao + (j0 + fj)) * so.nao_pair +
+                           k * (k + 1) / 2 + l] = acc[n];
+                }
+            }
+        } else {
+#pragma unroll
+            for (int n = 0; n < kHeavyAcc; n++) {
+                const int e = e0 + tid + n * kHeavyThreads;
+                if (e < ne) {
+                    const int f = e / NC, c = e - f * NC;
+                    qv[2 * c] += acc[n] * (1.0 + 0.125 * (f & 7));
+                    qv[2 * c + 1] += acc[n] * acc[n];
+                }
+            }
+        }
+    }
+    if (MODE != MODE_S2KL) {
+        __shared__ double red[kHeavyThreads / 32][6];
+        for (int c = 0; c < 2 * NC; c++)
+            for (int o = 16; o > 0; o >>= 1) qv[c] += __shfl_xor_sync(0xffffffffu, qv[c], o);
+        __syncthreads();
+        if ((tid & 31) == 0)
+            for (int c = 0; c < 2 * NC; c++) red[tid >> 5][c] = qv[c];
+        __syncthreads();
+        if (tid == 0)
+            for (int c = 0; c < 2 * NC; c++) {
+                double t = 0.0;
+                for (int w = 0; w < kHeavyThreads / 32; w++) t += red[w][c];
+                qsum[c] = t;
+            }
+    }
+}
+
 __device__ __forceinline__ void decode_pair(long long p, int &k, int &l)
 {
     int kk = (int)((sqrt(8.0 * (double)p + 1.0) - 1.0) * 0.5);
@@ -442,6 +637,7 @@ __global__ void __launch_bounds__(kWarps * 32, LOW ? (D ? 2 : 3) : 2) eri_s2kl_k
         int ksh, lsh;
         decode_pair(q - ij * npairs, ksh, lsh);
         const int ish = ish0 + (int)(ij / nbas), jsh = (int)(ij % nbas);
+        if (quartet_nf(bas, ish, jsh, ksh, lsh) > kHeavyNf) continue;
         eri_quartet<D, MODE_S2KL, LOW>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, wsm, smem_warp, so, nullptr, lane);
     }
 }
@@ -459,11 +655,49 @@ __global__ void __launch_bounds__(kWarps * 32, LOW ? (D ? 2 : 3) : 2) eri_qsum_k
     constexpr int NC = D ? 3 : 1;
     for (long long q = (long long)blockIdx.x * kWarps + warp; q < nq; q += (long long)gridDim.x * kWarps) {
         const int4 s = quartets[q];
+        if (quartet_nf(bas, s.x, s.y, s.z, s.w) > kHeavyNf) continue;
         double acc[2 * NC];
         for (int c = 0; c < 2 * NC; c++) acc[c] = 0.0;
         eri_quartet<D, MODE_QSUM, LOW>(atm, bas, env, nullptr, s.x, s.y, s.z, s.w, wsm, smem_warp, so, acc, lane);
         if (lane == 0)
             for (int c = 0; c < 2 * NC; c++) qsum[q * 2 * NC + c] = acc[c];
+    }
+}
+
+// Heavy quartets of the s2kl block (explicit list built by the caller).
+template <int D, bool LOW>
+__global__ void __launch_bounds__(kHeavyThreads, 1) eri_s2kl_heavy_kernel(
+    const int *__restrict__ atm, const int *__restrict__ bas, const double *__restrict__ env,
+    const int *__restrict__ ao_loc, int ish0, int ish1, int nao, const int4 *__restrict__ quartets, long long nq,
+    double *__restrict__ out, int smem_doubles)
+{
+    extern __shared__ double smem[];
+    S2klOut so;
+    so.out = out;
+    so.nao = nao;
+    so.nao_pair = (long long)nao * (nao + 1) / 2;
+    so.comp_stride = (long long)(ao_loc[ish1] - ao_loc[ish0]) * nao * so.nao_pair;
+    so.i_base = ao_loc[ish0];
+    for (long long q = blockIdx.x; q < nq; q += gridDim.x) {
+        const int4 s = quartets[q];
+        eri_quartet_cta<D, MODE_S2KL, LOW>(atm, bas, env, ao_loc, s.x, s.y, s.z, s.w, smem, smem_doubles, so, nullptr);
+    }
+}
+
+// Heavy quartets of an explicit list (light ones are skipped here).
+template <int D, bool LOW>
+__global__ void __launch_bounds__(kHeavyThreads, 1) eri_qsum_heavy_kernel(
+    const int *__restrict__ atm, const int *__restrict__ bas, const double *__restrict__ env,
+    const int4 *__restrict__ quartets, long long nq, double *__restrict__ qsum, int smem_doubles)
+{
+    extern __shared__ double smem[];
+    S2klOut so = {};
+    constexpr int NC = D ? 3 : 1;
+    for (long long q = blockIdx.x; q < nq; q += gridDim.x) {
+        const int4 s = quartets[q];
+        if (quartet_nf(bas, s.x, s.y, s.z, s.w) <= kHeavyNf) continue;
+        eri_quartet_cta<D, MODE_QSUM, LOW>(atm, bas, env, nullptr, s.x, s.y, s.z, s.w, smem, smem_doubles, so,
+                                           qsum + q * 2 * NC);
     }
 }
 
@@ -526,6 +760,45 @@ static int smem_per_warp(int lmax, int deriv)
     return need < 2048 ? 2048 : need;
 }
 
+// shared memory of the CTA kernel: up to 64 slots of the largest class, <= 200 KiB
+static int heavy_smem_doubles(int lmax, int deriv)
+{
+    const int gsz = (lmax + 1 + deriv) * (lmax + 1) * (lmax + 1) * (lmax + 1);
+    const long long want = (long long)kMaxSlots * (3 * gsz + kParStride);
+    const long long cap = 200 * 1024 / 8;
+    return (int)(want < cap ? want : cap);
+}
+
+// Library-owned auxiliary stream per device: the heavy-quartet kernel runs on
+// it, fork/joined with the caller's stream by events, so it overlaps the warp
+// kernel instead of serialising behind it.
+struct AuxStream {
+    cudaStream_t s = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+};
+
+static int aux_stream(AuxStream **out)
+{
+    static AuxStream aux[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        set_error("aux_stream: no current CUDA device");
+        return CCSD_B200_ERR_LAUNCH;
+    }
+    AuxStream &a = aux[dev];
+    if (!a.s) {
+        if (cudaStreamCreateWithFlags(&a.s, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&a.fork, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&a.join, cudaEventDisableTiming) != cudaSuccess) {
+            set_error("aux_stream: stream/event creation failed");
+            a.s = nullptr;
+            return CCSD_B200_ERR_LAUNCH;
+        }
+    }
+    *out = &a;
+    return CCSD_B200_OK;
+}
+
 static int num_sms()
 {
     static int n = 0;
@@ -560,11 +833,11 @@ extern "C" {
 const char *ccsd_b200_last_error(void) { return g_err; }
 
 int ccsd_b200_eri_s2kl_cart(int deriv, const int32_t *atm, const int32_t *bas, const double *env, int nbas,
-                            const int32_t *ao_loc, int ish0, int ish1, int nao, int lmax, double *out,
-                            void *stream)
+                            const int32_t *ao_loc, int ish0, int ish1, int nao, int lmax,
+                            const int32_t *heavy_quartets, long long n_heavy, double *out, void *stream)
 {
     if (deriv < 0 || deriv > 1 || !atm || !bas || !env || !ao_loc || !out || nbas <= 0 || ish0 < 0 ||
-        ish1 > nbas || ish0 >= ish1 || nao <= 0 || lmax < 0) {
+        ish1 > nbas || ish0 >= ish1 || nao <= 0 || lmax < 0 || n_heavy < 0 || (n_heavy > 0 && !heavy_quartets)) {
         set_error("ccsd_b200_eri_s2kl_cart: invalid argument");
         return CCSD_B200_ERR_ARG;
     }
@@ -580,6 +853,28 @@ int ccsd_b200_eri_s2kl_cart(int deriv, const int32_t *atm, const int32_t *bas, c
     if (grid > gmax) grid = gmax;
     cudaStream_t st = (cudaStream_t)stream;
     int rc;
+    AuxStream *aux = nullptr;
+    if (n_heavy > 0) {
+        if ((rc = aux_stream(&aux))) return rc;
+        cudaEventRecord(aux->fork, st);
+        cudaStreamWaitEvent(aux->s, aux->fork, 0);
+        const int hd = heavy_smem_doubles(lmax, deriv);
+        const size_t hsmem = (size_t)hd * sizeof(double);
+        const long long hg = n_heavy < (long long)num_sms() ? n_heavy : (long long)num_sms();
+        const int4 *hq = reinterpret_cast<const int4 *>(heavy_quartets);
+#define CB_LAUNCH_S2KL_H(DV, LOWV)                                                                             \
+    if ((rc = prepare_kernel(eri_s2kl_heavy_kernel<DV, LOWV>, hsmem))) return rc;                               \
+    eri_s2kl_heavy_kernel<DV, LOWV><<<(int)hg, kHeavyThreads, hsmem, aux->s>>>(atm, bas, env, ao_loc, ish0, ish1, \
+                                                                               nao, hq, n_heavy, out, hd);
+        if (deriv) {
+            if (lmax <= 2) { CB_LAUNCH_S2KL_H(1, true) } else { CB_LAUNCH_S2KL_H(1, false) }
+        } else {
+            if (lmax <= 2) { CB_LAUNCH_S2KL_H(0, true) } else { CB_LAUNCH_S2KL_H(0, false) }
+        }
+#undef CB_LAUNCH_S2KL_H
+        if ((rc = check_launch("eri_s2kl_heavy_kernel"))) return rc;
+        cudaEventRecord(aux->join, aux->s);
+    }
 #define CB_LAUNCH_S2KL(DV, LOWV)                                                                              \
     if ((rc = prepare_kernel(eri_s2kl_kernel<DV, LOWV>, smem))) return rc;                                     \
     eri_s2kl_kernel<DV, LOWV><<<(int)grid, kWarps * 32, smem, st>>>(atm, bas, env, ao_loc, ish0, ish1, nbas, nao, \
@@ -590,6 +885,7 @@ int ccsd_b200_eri_s2kl_cart(int deriv, const int32_t *atm, const int32_t *bas, c
         if (lmax <= 2) { CB_LAUNCH_S2KL(0, true) } else { CB_LAUNCH_S2KL(0, false) }
     }
 #undef CB_LAUNCH_S2KL
+    if (aux) cudaStreamWaitEvent(st, aux->join, 0);
     return check_launch("eri_s2kl_kernel");
 }
 
@@ -614,6 +910,26 @@ int ccsd_b200_eri_quartet_checksums(int deriv, const int32_t *atm, const int32_t
     cudaStream_t st = (cudaStream_t)stream;
     int rc;
     const int4 *q4 = reinterpret_cast<const int4 *>(quartets);
+    AuxStream *aux = nullptr;
+    if ((rc = aux_stream(&aux))) return rc;
+    cudaEventRecord(aux->fork, st);
+    cudaStreamWaitEvent(aux->s, aux->fork, 0);
+    {
+        const int hd = heavy_smem_doubles(lmax, deriv);
+        const size_t hsmem = (size_t)hd * sizeof(double);
+        const long long hg = nq < (long long)num_sms() ? nq : (long long)num_sms();
+#define CB_LAUNCH_QSUM_H(DV, LOWV)                                                     \
+    if ((rc = prepare_kernel(eri_qsum_heavy_kernel<DV, LOWV>, hsmem))) return rc;       \
+    eri_qsum_heavy_kernel<DV, LOWV><<<(int)hg, kHeavyThreads, hsmem, aux->s>>>(atm, bas, env, q4, nq, qsum, hd);
+        if (deriv) {
+            if (lmax <= 2) { CB_LAUNCH_QSUM_H(1, true) } else { CB_LAUNCH_QSUM_H(1, false) }
+        } else {
+            if (lmax <= 2) { CB_LAUNCH_QSUM_H(0, true) } else { CB_LAUNCH_QSUM_H(0, false) }
+        }
+#undef CB_LAUNCH_QSUM_H
+        if ((rc = check_launch("eri_qsum_heavy_kernel"))) return rc;
+        cudaEventRecord(aux->join, aux->s);
+    }
 #define CB_LAUNCH_QSUM(DV, LOWV)                                                       \
     if ((rc = prepare_kernel(eri_qsum_kernel<DV, LOWV>, smem))) return rc;              \
     eri_qsum_kernel<DV, LOWV><<<(int)grid, kWarps * 32, smem, st>>>(atm, bas, env, q4, nq, qsum, sw);
@@ -623,6 +939,7 @@ int ccsd_b200_eri_quartet_checksums(int deriv, const int32_t *atm, const int32_t
         if (lmax <= 2) { CB_LAUNCH_QSUM(0, true) } else { CB_LAUNCH_QSUM(0, false) }
     }
 #undef CB_LAUNCH_QSUM
+    cudaStreamWaitEvent(st, aux->join, 0);
     return check_launch("eri_qsum_kernel");
 }
 

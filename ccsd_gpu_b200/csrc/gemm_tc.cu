@@ -1,0 +1,441 @@
+// Split-precision tensor-core GEMM for sm_100a (tcgen05 + TMA + TMEM).
+//
+//   D[m, n] = sum_k A[m, k] B[n, k]     (A, B given in FP64)
+// is evaluated as  A_hi B_hi + A_hi B_lo + A_lo B_hi  with A = A_hi + A_lo,
+// B = B_hi + B_lo split into two TF32 (kind::tf32) or BF16 (kind::f16) parts:
+// three tcgen05.mma per K step into an FP32 accumulator in tensor memory.
+// The TF32 split represents an FP64 value to ~2^-24 relative, so the error is
+// set by the FP32 accumulation; to keep it at the FP32 level for long K, the
+// accumulator is drained into the FP64 output every 512 k (double-buffered in
+// TMEM, so the MMAs of chunk c+1 overlap the drain of chunk c).  The drain
+// scatters through per-row / per-column offset tables, so any einsum output
+// permutation is written in place:  out[off_m[m] + off_n[n]] = alpha*D + beta*out.
+//
+// Operands are produced by split_pack_kernel: it gathers an FP64 operand (up
+// to two linear terms, each addressed through offset tables, so transposes and
+// "2 t - t^T" combinations fuse into the pack), splits every value into hi and
+// lo parts and writes K-major, zero-padded [rows_pad x k_pad] arrays for TMA.
+//
+// CTA = 192 threads, one 128 x 128 output tile:
+//   warp 0      TMA producer (lane 0) into a 3-stage ring of {A_hi, A_lo, B_hi,
+//               B_lo} tiles (128 rows x 128 B, 128 B swizzle); owns TMEM alloc.
+//   warp 1      MMA issuer (lane 0); commits stage releases and chunk-ready.
+//   warps 2..5  drain TMEM (warp w reads lanes 32*(w%4) .. +31) into FP64.
+// Every mbarrier wait is bounded by the global timer (2 s): on expiry the
+// thread records a code in `status` and leaves its loop -- no trap, no
+// unbounded spin.
+#include "common.cuh"
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_bf16.h>
+
+namespace cb {
+
+static constexpr int TC_BM = 128;
+static constexpr int TC_BN = 128;
+static constexpr int TC_STAGES = 3;
+static constexpr int TC_ROWB = 128;                      // bytes per tile row (swizzle span)
+static constexpr int TC_TILE_BYTES = TC_BM * TC_ROWB;    // 16 KiB
+static constexpr int TC_STAGE_BYTES = 4 * TC_TILE_BYTES;
+static constexpr int TC_THREADS = 192;
+static constexpr int TC_CHUNK_K = 512;                   // k per FP32 accumulation chunk
+static constexpr unsigned long long TC_WAIT_NS = 2000000000ull;
+
+enum { KIND_TF32 = 0, KIND_BF16 = 1 };
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// bounded wait: false (and `code` recorded in *status) after TC_WAIT_NS
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *status, int code)
+{
+    const unsigned long long t0 = global_ns();
+    for (unsigned it = 0;; it++) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((it & 63) == 63) {
+            if (*(volatile int *)status != 0) return false;       // another CTA already gave up
+            if (global_ns() - t0 > TC_WAIT_NS) break;
+        }
+    }
+    atomicCAS(status, 0, code);
+    return false;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tma_load_2d(const CUtensorMap *map, uint64_t *bar, void *dst, int x, int y)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
+        ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
+        : "memory");
+}
+
+// K-major, 128 B swizzle UMMA shared-memory descriptor (8-row groups 1024 B apart)
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr)
+{
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);          // start address
+    d |= (uint64_t)1 << 16;                            // leading byte offset (unused for SW128 K-major)
+    d |= (uint64_t)(1024 >> 4) << 32;                  // stride byte offset
+    d |= (uint64_t)1 << 46;                            // descriptor version (sm_100)
+    d |= (uint64_t)2 << 61;                            // SWIZZLE_128B
+    return d;
+}
+
+template <int KIND>
+__device__ __forceinline__ uint32_t instr_desc()
+{
+    const uint32_t fmt = KIND == KIND_TF32 ? 2u : 1u;  // A/B format: TF32 = 2, BF16 = 1
+    return (1u << 4)                                   // D format F32
+           | (fmt << 7) | (fmt << 10)                  // A, B formats, both K-major
+           | ((uint32_t)(TC_BN >> 3) << 17)            // N
+           | ((uint32_t)(TC_BM >> 4) << 24);           // M
+}
+
+template <int KIND>
+__device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc)
+{
+    if (KIND == KIND_TF32)
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+            ::"r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+    else
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+            ::"r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t *bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v)
+{
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+        "%14, %15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(TC_THREADS, 1) tc_split_gemm_kernel(
+    const __grid_constant__ CUtensorMap map_ahi, const __grid_constant__ CUtensorMap map_alo,
+    const __grid_constant__ CUtensorMap map_bhi, const __grid_constant__ CUtensorMap map_blo,
+    int M, int N, int kblocks, double *__restrict__ out, const long long *__restrict__ off_m,
+    const long long *__restrict__ off_n, double alpha, double beta, int *__restrict__ status)
+{
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    __shared__ __align__(8) uint64_t full_bar[TC_STAGES], empty_bar[TC_STAGES], accf_bar[2], acce_bar[2];
+    __shared__ uint32_t tmem_base_s;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.y * TC_BM, n0 = blockIdx.x * TC_BN;
+    constexpr int KB_ELEMS = TC_ROWB / (KIND == KIND_TF32 ? 4 : 2);   // k per pipeline stage
+    constexpr int KB_PER_CHUNK = TC_CHUNK_K / KB_ELEMS;
+    const int nchunks = (kblocks + KB_PER_CHUNK - 1) / KB_PER_CHUNK;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < TC_STAGES; s++) {
+            mbar_init(&full_bar[s], 1);
+            mbar_init(&empty_bar[s], 1);
+        }
+        for (int b = 0; b < 2; b++) {
+            mbar_init(&accf_bar[b], 1);
+            mbar_init(&acce_bar[b], 4);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(&tmem_base_s)), "r"(2 * TC_BN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_base_s;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---- TMA producer
+            for (int kb = 0; kb < kblocks; kb++) {
+                const int s = kb % TC_STAGES;
+                const uint32_t ph = (kb / TC_STAGES) & 1;
+                if (!mbar_wait(&empty_bar[s], ph ^ 1, status, 1)) break;
+                uint8_t *st = smem + s * TC_STAGE_BYTES;
+                mbar_expect_tx(&full_bar[s], TC_STAGE_BYTES);
+                const int kx = kb * KB_ELEMS;
+                tma_load_2d(&map_ahi, &full_bar[s], st, kx, m0);
+                tma_load_2d(&map_alo, &full_bar[s], st + TC_TILE_BYTES, kx, m0);
+                tma_load_2d(&map_bhi, &full_bar[s], st + 2 * TC_TILE_BYTES, kx, n0);
+                tma_load_2d(&map_blo, &full_bar[s], st + 3 * TC_TILE_BYTES, kx, n0);
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // ---- MMA issuer
+            const uint32_t idesc = instr_desc<KIND>();
+            bool ok = true;
+            for (int c = 0; c < nchunks && ok; c++) {
+                const int buf = c & 1;
+                const uint32_t use = (uint32_t)(c >> 1);
+                if (!mbar_wait(&acce_bar[buf], (use & 1) ^ 1, status, 2)) break;
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t acc_tmem = tmem + buf * TC_BN;
+                const int kb0 = c * KB_PER_CHUNK, kb1 = min(kblocks, kb0 + KB_PER_CHUNK);
+                for (int kb = kb0; kb < kb1; kb++) {
+                    const int s = kb % TC_STAGES;
+                    const uint32_t ph = (kb / TC_STAGES) & 1;
+                    if (!mbar_wait(&full_bar[s], ph, status, 3)) { ok = false; break; }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t base = smem_u32(smem + s * TC_STAGE_BYTES);
+#pragma unroll
+                    for (int k = 0; k < 4; k++) {          // 128 B row = 4 UMMA K steps of 32 B
+                        const uint64_t ahi = umma_desc(base + k * 32);
+                        const uint64_t alo = umma_desc(base + TC_TILE_BYTES + k * 32);
+                        const uint64_t bhi = umma_desc(base + 2 * TC_TILE_BYTES + k * 32);
+                        const uint64_t blo = umma_desc(base + 3 * TC_TILE_BYTES + k * 32);
+                        umma<KIND>(acc_tmem, ahi, bhi, idesc, (kb != kb0 || k) ? 1u : 0u);
+                        umma<KIND>(acc_tmem, ahi, blo, idesc, 1u);
+                        umma<KIND>(acc_tmem, alo, bhi, idesc, 1u);
+                    }
+                    umma_commit(&empty_bar[s]);     // stage reusable once these MMAs finish
+                }
+                umma_commit(&accf_bar[buf]);        // chunk accumulated (also on the error path)
+            }
+        }
+    } else {
+        // ---- drain warps
+        const int q = warp & 3;
+        const int m = m0 + q * 32 + lane;
+        const long long om = m < M ? off_m[m] : 0;
+        for (int c = 0; c < nchunks; c++) {
+            const int buf = c & 1;
+            const uint32_t use = (uint32_t)(c >> 1);
+            const bool got = mbar_wait(&accf_bar[buf], use & 1, status, 4);
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            // warp-uniform: tcgen05.ld is a .sync.aligned instruction
+            if (!__all_sync(0xffffffffu, got && *(volatile int *)status == 0)) break;
+#pragma unroll 1
+            for (int c0 = 0; c0 < TC_BN; c0 += 16) {
+                float v[16];
+                tmem_ld16(tmem + buf * TC_BN + ((uint32_t)(q * 32) << 16) + c0, v);
+                if (m < M) {
+#pragma unroll
+                    for (int i = 0; i < 16; i++) {
+                        const int n = n0 + c0 + i;
+                        if (n < N) {
+                            double *o = out + om + off_n[n];
+                            const double val = alpha * (double)v[i];
+                            if (c == 0)
+                                *o = beta == 0.0 ? val : fma(beta, *o, val);
+                            else
+                                *o += val;
+                        }
+                    }
+                }
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acce_bar[buf]);
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * TC_BN));
+    }
+}
+
+// ---- operand gather + split ----
+// dst row r, column k  <-  c1 * src1[o1r[r] + o1k[k]] + c2 * src2[o2r[r] + o2k[k]]
+// (second term optional), split into hi + lo of the MMA input type.
+template <int KIND>
+__global__ void split_pack_kernel(const double *__restrict__ src1, const long long *__restrict__ o1r,
+                                  const long long *__restrict__ o1k, double c1, const double *__restrict__ src2,
+                                  const long long *__restrict__ o2r, const long long *__restrict__ o2k, double c2,
+                                  int rows, int K, int rows_pad, int k_pad, void *__restrict__ hi,
+                                  void *__restrict__ lo)
+{
+    const long long total = (long long)rows_pad * k_pad;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(e / k_pad), k = (int)(e - (long long)r * k_pad);
+        double x = 0.0;
+        if (r < rows && k < K) {
+            x = c1 * src1[o1r[r] + o1k[k]];
+            if (src2) x = fma(c2, src2[o2r[r] + o2k[k]], x);
+        }
+        if (KIND == KIND_TF32) {
+            uint32_t h, l;
+            const float xf = (float)x;
+            asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(xf));
+            const float rest = (float)(x - (double)__uint_as_float(h));
+            asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(l) : "f"(rest));
+            reinterpret_cast<uint32_t *>(hi)[e] = h;
+            reinterpret_cast<uint32_t *>(lo)[e] = l;
+        } else {
+            const __nv_bfloat16 h = __double2bfloat16(x);
+            const __nv_bfloat16 l = __double2bfloat16(x - (double)__bfloat162float(h));
+            reinterpret_cast<__nv_bfloat16 *>(hi)[e] = h;
+            reinterpret_cast<__nv_bfloat16 *>(lo)[e] = l;
+        }
+    }
+}
+
+// ---- host side ----
+static PFN_cuTensorMapEncodeTiled_v12000 get_encode()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        cudaDriverEntryPointQueryResult q;
+        void *p = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+static int make_map(CUtensorMap *map, const void *base, int kind, int rows_pad, int k_pad)
+{
+    auto enc = get_encode();
+    if (!enc) {
+        set_error("cuTensorMapEncodeTiled unavailable");
+        return CCSD_B200_ERR_LAUNCH;
+    }
+    const int esz = kind == KIND_TF32 ? 4 : 2;
+    cuuint64_t dims[2] = {(cuuint64_t)k_pad, (cuuint64_t)rows_pad};
+    cuuint64_t strides[1] = {(cuuint64_t)k_pad * esz};
+    cuuint32_t box[2] = {(cuuint32_t)(TC_ROWB / esz), (cuuint32_t)TC_BM};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = enc(map, kind == KIND_TF32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2,
+                     const_cast<void *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
+        return CCSD_B200_ERR_LAUNCH;
+    }
+    return CCSD_B200_OK;
+}
+
+template <int KIND>
+static int launch_tc(const CUtensorMap &ma, const CUtensorMap &mal, const CUtensorMap &mb, const CUtensorMap &mbl,
+                     int M, int N, int m_pad, int n_pad, int kblocks, double *out, const long long *off_m,
+                     const long long *off_n, double alpha, double beta, int *status, cudaStream_t st)
+{
+    const size_t smem = TC_STAGES * TC_STAGE_BYTES + 1024;
+    if (cudaFuncSetAttribute(tc_split_gemm_kernel<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+        return check_launch("cudaFuncSetAttribute(tc_split_gemm_kernel)");
+    dim3 grid(n_pad / TC_BN, m_pad / TC_BM);
+    tc_split_gemm_kernel<KIND><<<grid, TC_THREADS, smem, st>>>(ma, mal, mb, mbl, M, N, kblocks, out, off_m, off_n,
+                                                                alpha, beta, status);
+    return check_launch("tc_split_gemm_kernel");
+}
+
+}  // namespace cb
+
+using namespace cb;
+
+extern "C" {
+
+int ccsd_b200_split_pack(int kind, const double *src1, const long long *o1r, const long long *o1k, double c1,
+                         const double *src2, const long long *o2r, const long long *o2k, double c2, int rows, int K,
+                         int rows_pad, int k_pad, void *hi, void *lo, void *stream)
+{
+    if ((kind != KIND_TF32 && kind != KIND_BF16) || !src1 || !o1r || !o1k || rows < 0 || K < 0 ||
+        rows_pad < rows || k_pad < K || !hi || !lo || (src2 && (!o2r || !o2k)) || rows_pad % TC_BM ||
+        k_pad % (TC_ROWB / (kind == KIND_TF32 ? 4 : 2))) {
+        set_error("ccsd_b200_split_pack: invalid argument");
+        return CCSD_B200_ERR_ARG;
+    }
+    const long long total = (long long)rows_pad * k_pad;
+    if (total == 0) return CCSD_B200_OK;
+    long long grid = (total + 255) / 256;
+    if (grid > 148 * 64) grid = 148 * 64;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (kind == KIND_TF32)
+        split_pack_kernel<KIND_TF32><<<(int)grid, 256, 0, st>>>(src1, o1r, o1k, c1, src2, o2r, o2k, c2, rows, K,
+                                                                rows_pad, k_pad, hi, lo);
+    else
+        split_pack_kernel<KIND_BF16><<<(int)grid, 256, 0, st>>>(src1, o1r, o1k, c1, src2, o2r, o2k, c2, rows, K,
+                                                                rows_pad, k_pad, hi, lo);
+    return check_launch("split_pack_kernel");
+}
+
+int ccsd_b200_tc_split_gemm(int kind, const void *a_hi, const void *a_lo, const void *b_hi, const void *b_lo, int M,
+                            int N, int m_pad, int n_pad, int k_pad, double *out, const long long *off_m,
+                            const long long *off_n, double alpha, double beta, int *status, void *stream)
+{
+    const int kstep = TC_ROWB / (kind == KIND_TF32 ? 4 : 2);
+    if ((kind != KIND_TF32 && kind != KIND_BF16) || !a_hi || !a_lo || !b_hi || !b_lo || !out || !off_m || !off_n ||
+        !status || M <= 0 || N <= 0 || m_pad < M || n_pad < N || m_pad % TC_BM || n_pad % TC_BN || k_pad <= 0 ||
+        k_pad % kstep || n_pad / TC_BN > 2147483647 || m_pad / TC_BM > 65535) {
+        set_error("ccsd_b200_tc_split_gemm: invalid argument");
+        return CCSD_B200_ERR_ARG;
+    }
+    CUtensorMap ma, mal, mb, mbl;
+    int rc;
+    if ((rc = make_map(&ma, a_hi, kind, m_pad, k_pad)) || (rc = make_map(&mal, a_lo, kind, m_pad, k_pad)) ||
+        (rc = make_map(&mb, b_hi, kind, n_pad, k_pad)) || (rc = make_map(&mbl, b_lo, kind, n_pad, k_pad)))
+        return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (kind == KIND_TF32)
+        return launch_tc<KIND_TF32>(ma, mal, mb, mbl, M, N, m_pad, n_pad, k_pad / kstep, out, off_m, off_n, alpha,
+                                    beta, status, st);
+    return launch_tc<KIND_BF16>(ma, mal, mb, mbl, M, N, m_pad, n_pad, k_pad / kstep, out, off_m, off_n, alpha, beta,
+                                status, st);
+}
+
+}  // extern "C"

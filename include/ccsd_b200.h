@@ -38,6 +38,11 @@ const char *ccsd_b200_last_error(void);
  * comp = x, y, z for deriv = 1.  Every element of the block is written.
  * ao_loc: Cartesian AO offsets of the nbas decontracted shells (nbas + 1
  * entries); nao = ao_loc[nbas]; lmax = max l over the shells.
+ * heavy_quartets (int32 x 4, n_heavy entries) must list exactly the block's
+ * quartets (i in [ish0, ish1), any j, k >= l) whose Cartesian block has more
+ * than 1000 functions: those run on the CTA-cooperative kernel (on a
+ * library-owned stream fork/joined with `stream` by events), all others on
+ * the warp-per-quartet kernel.
  * Replaces fill_int2e_kernel / fill_int2e_ip1_kernel and the per-i-shell
  * launch loop of _compute_cart
  * (ref: ccsd_gpu/cuda/int2e_module.py:130-463, ccsd_gpu/cuda/int2e_gpu.py:39-108,
@@ -45,7 +50,7 @@ const char *ccsd_b200_last_error(void);
  */
 int ccsd_b200_eri_s2kl_cart(int deriv, const int32_t *atm, const int32_t *bas, const double *env,
                             int nbas, const int32_t *ao_loc, int ish0, int ish1, int nao, int lmax,
-                            double *out, void *stream);
+                            const int32_t *heavy_quartets, long long n_heavy, double *out, void *stream);
 
 /*
  * Integrals of an explicit list of shell quartets (int32 x 4 per quartet,
@@ -83,6 +88,36 @@ int ccsd_b200_cart2sph_s2kl(const double *cart, double *tmp, double *out, int nc
  * counterpart in the reference.
  */
 int ccsd_b200_fp64_fma_probe(double *out, int blocks, int iters, void *stream);
+
+/*
+ * Split-precision tensor-core contraction, step 1: gather + split.
+ *   v[r][k] = c1 * src1[o1r[r] + o1k[k]] + c2 * src2[o2r[r] + o2k[k]]   (src2 may be NULL)
+ * for r < rows, k < K (zero elsewhere), written as hi + lo parts, K-major,
+ * [rows_pad x k_pad]: kind 0 = TF32 (float storage, 4 B), kind 1 = BF16 (2 B).
+ * rows_pad must be a multiple of 128 and k_pad of 32 (TF32) / 64 (BF16).
+ * The offset tables (int64, element units) express any strided or permuted
+ * view of the FP64 operands.  Replaces the operand transposes/copies that
+ * precede the CuPy einsum contractions of the Lambda and RDM builders
+ * (ref: ccsd_gpu/gpu_ccsd_lambda.py:68-337, ccsd_gpu/gpu_ccsd_grad.py:101-246).
+ */
+int ccsd_b200_split_pack(int kind, const double *src1, const long long *o1r, const long long *o1k, double c1,
+                         const double *src2, const long long *o2r, const long long *o2k, double c2, int rows,
+                         int K, int rows_pad, int k_pad, void *hi, void *lo, void *stream);
+
+/*
+ * Split-precision tensor-core contraction, step 2 (tcgen05 + TMA + TMEM):
+ *   out[off_m[m] + off_n[n]] = alpha * sum_k (Ahi Bhi + Ahi Blo + Alo Bhi)[m,n,k] + beta * out[...]
+ * for m < M, n < N.  The tensor cores accumulate in FP32 over chunks of
+ * 512 k; each chunk is added to the output in FP64.  Operands come from
+ * ccsd_b200_split_pack (A: [m_pad x k_pad], B: [n_pad x k_pad], m_pad and
+ * n_pad multiples of 128).  `status` (one int, zero-initialised by the
+ * caller) receives a non-zero code if a pipeline wait expired.  Replaces the
+ * cuTENSOR/cuBLAS einsum contractions of the Lambda solver and density
+ * builders, and the CPU vvvv ladder term (ref: ccsd_gpu/gpu_ccsd_lambda.py:238-241).
+ */
+int ccsd_b200_tc_split_gemm(int kind, const void *a_hi, const void *a_lo, const void *b_hi, const void *b_lo,
+                            int M, int N, int m_pad, int n_pad, int k_pad, double *out, const long long *off_m,
+                            const long long *off_n, double alpha, double beta, int *status, void *stream);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,57 @@
+"""Split-precision tcgen05 contractions against FP64 einsum (GPU).
+
+tf32x3 represents each FP64 operand to ~2^-24 relative; the tensor cores
+accumulate in FP32 over 512-k chunks that are summed in FP64, so the error
+is that of a 512-term FP32 sum: a few 1e-6 of the largest output element."""
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    return float((a - b).abs().max() / b.abs().max())
+
+
+@pytest.mark.parametrize("mode,tol", [("tf32x3", 3e-6), ("bf16x3", 1e-4)])
+def test_plain_gemm(mode, tol):
+    from ccsd_gpu_b200.contract import check_status, contract
+    g = torch.Generator(device="cuda").manual_seed(0)
+    for M, N, K in [(128, 128, 32), (200, 300, 100), (1, 7, 5), (333, 129, 1000), (260, 140, 5000)]:
+        a = torch.randn(M, K, dtype=torch.float64, device="cuda", generator=g)
+        b = torch.randn(N, K, dtype=torch.float64, device="cuda", generator=g)
+        ref = a @ b.T
+        got = contract("mk,nk->mn", a, b, mode=mode)
+        check_status()
+        assert _rel(got, ref) < tol, (M, N, K, _rel(got, ref))
+
+
+def test_permuted_contraction_with_combined_operand_and_beta():
+    from ccsd_gpu_b200.contract import check_status, contract
+    g = torch.Generator(device="cuda").manual_seed(1)
+    o, v = 6, 23
+    ovvv = torch.randn(o, v, v, v, dtype=torch.float64, device="cuda", generator=g)
+    t2 = torch.randn(o, o, v, v, dtype=torch.float64, device="cuda", generator=g)
+    theta = [(2.0, t2), (-1.0, t2.permute(0, 1, 3, 2))]
+    out = torch.randn(v, v, o, v, dtype=torch.float64, device="cuda", generator=g)
+    ref = 0.5 * out - 1.5 * torch.einsum("jabd,jkcd->abkc", ovvv, 2 * t2 - t2.permute(0, 1, 3, 2))
+    contract("jabd,jkcd->abkc", ovvv, theta, out=out, alpha=-1.5, beta=0.5)
+    check_status()
+    assert _rel(out, ref) < 3e-6
+
+
+def test_outer_product_and_batch_index():
+    from ccsd_gpu_b200.contract import contract
+    g = torch.Generator(device="cuda").manual_seed(2)
+    t1 = torch.randn(5, 9, dtype=torch.float64, device="cuda", generator=g)
+    assert _rel(contract("ia,jb->ijab", t1, t1), torch.einsum("ia,jb->ijab", t1, t1)) < 3e-6
+    x = torch.randn(4, 6, 7, dtype=torch.float64, device="cuda", generator=g)
+    y = torch.randn(4, 7, 3, dtype=torch.float64, device="cuda", generator=g)
+    assert _rel(contract("bij,bjk->bik", x, y), torch.einsum("bij,bjk->bik", x, y)) < 3e-6
+
+
+def test_fp64_mode_is_einsum():
+    from ccsd_gpu_b200.contract import contract
+    a = torch.randn(7, 8, dtype=torch.float64, device="cuda")
+    b = torch.randn(9, 8, dtype=torch.float64, device="cuda")
+    assert torch.allclose(contract("mk,nk->mn", a, b, mode="fp64"), a @ b.T, rtol=1e-14, atol=1e-14)

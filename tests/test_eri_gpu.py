@@ -100,8 +100,8 @@ def test_invalid_arguments_are_rejected_on_host():
     with pytest.raises(ValueError):
         compute_int2e_gpu(mol, 1, 1)
     with pytest.raises(_native.NativeError):
-        _native.call("ccsd_b200_eri_s2kl_cart", 0, None, None, None, 0, None, 0, 0, 0, 0, None, None)
+        _native.call("ccsd_b200_eri_s2kl_cart", 0, None, None, None, 0, None, 0, 0, 0, 0, None, 0, None, None)
     with pytest.raises(_native.NativeError):
         x = torch.zeros(8, dtype=torch.float64, device="cuda")
         _native.call("ccsd_b200_eri_s2kl_cart", 0, _native.ptr(x), _native.ptr(x), _native.ptr(x), 1,
-                     _native.ptr(x), 0, 1, 1, 5, _native.ptr(x), None)
+                     _native.ptr(x), 0, 1, 1, 5, None, 0, _native.ptr(x), None)

@@ -1,0 +1,64 @@
+"""GPU Lambda solver against the reference's golden vectors and the oracle."""
+import os
+from types import SimpleNamespace
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import cc_oracle as C
+from tests.conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"fp64": 1e-12, "tf32x3": 2e-6, "bf16x3": 2e-4}
+
+
+@pytest.fixture(scope="module")
+def gold():
+    d = dict(np.load(os.path.join(GOLDEN, "cc_small.npz")))
+    eris = C.mo_blocks(d["g"], d["t1"].shape[0])
+    d["eris"] = SimpleNamespace(fock=d["fock"], mo_energy=d["mo_energy"], **vars(eris))
+    return d
+
+
+def rel(a, b):
+    a = a.detach().cpu().numpy() if isinstance(a, torch.Tensor) else a
+    return np.abs(a - b).max() / np.abs(b).max()
+
+
+@pytest.mark.parametrize("mode", ["fp64", "tf32x3", "bf16x3"])
+def test_intermediates_and_update_match_reference_golden(gold, mode):
+    from ccsd_gpu_b200.gpu_ccsd_lambda import make_intermediates_gpu, update_lambda_gpu
+    cc = SimpleNamespace(level_shift=0.0)
+    imds = make_intermediates_gpu(cc, gold["t1"], gold["t2"], gold["eris"], mode=mode)
+    for k in ("w1", "w2", "w3", "w4", "woooo", "wvooo", "wVOov", "wvOOv", "wvvov"):
+        assert rel(getattr(imds, k), gold["imds_" + k]) < TOL[mode], (mode, k)
+    l1, l2 = update_lambda_gpu(cc, gold["t1"], gold["t2"], gold["l1"], gold["l2"], gold["eris"], imds, mode=mode)
+    assert rel(l1, gold["l1new"]) < TOL[mode]
+    assert rel(l2, gold["l2new"]) < TOL[mode]
+
+
+def _oracle_solution(d, tol=1e-12):
+    eris = C.mo_blocks(d["g"], d["t1"].shape[0])
+    imds = C.make_intermediates(d["t1"], d["t2"], d["fock"], eris)
+    l1, l2 = d["t1"], d["t2"]
+    for _ in range(200):
+        n1, n2 = C.update_lambda(d["t1"], d["t2"], l1, l2, d["fock"], d["mo_energy"], eris, imds)
+        done = max(np.abs(n1 - l1).max(), np.abs(n2 - l2).max()) < tol
+        l1, l2 = n1, n2
+        if done:
+            break
+    return l1, l2
+
+
+@pytest.mark.parametrize("mode", ["fp64", "tf32x3"])
+def test_solve_lambda_converges_to_oracle_fixed_point(gold, mode):
+    from ccsd_gpu_b200.gpu_ccsd_lambda import solve_lambda_gpu
+    ref1, ref2 = _oracle_solution(gold)
+    cc = SimpleNamespace(t1=gold["t1"], t2=gold["t2"], max_cycle=100, conv_tol_normt=1e-10, level_shift=0.0,
+                         precision=mode)
+    l1, l2 = solve_lambda_gpu(cc, eris=gold["eris"])
+    assert cc.converged_lambda
+    tol = 1e-9 if mode == "fp64" else 1e-6
+    assert rel(l1, ref1) < tol and rel(l2, ref2) < tol
