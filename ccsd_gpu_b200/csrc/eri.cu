@@ -972,3 +972,81 @@ int ccsd_b200_cart2sph_s2kl(const double *cart, double *tmp, double *out, int nc
 }
 
 }  // extern "C"
+
+// ---- Spherical transform for callers that cannot allocate device memory ----
+//
+// Some callers cannot call cudaMalloc: a host application that hands this
+// library a device it has already carved up with its own pool allocator, or
+// one that forbids allocation once its time step is running (cudaMalloc can
+// synchronise the device and stall the work other components have queued).
+// They can pass their input and output buffers but have nowhere to put the
+// transform's intermediate.  This variant keeps that intermediate in a
+// fixed, file-scope device array instead.
+//   * The array holds kC2sScratchDoubles doubles (32 MiB).  Every GPU that
+//     loads the library reserves it until the process exits.
+//   * Host code cannot use the array's name as a device address, so the
+//     first call on each device (with that device current) looks the address
+//     up with cudaGetSymbolAddress and caches it.  Make that first call before
+//     any stream capture.
+//   * All calls share the one array.  Nothing in it has to start at zero:
+//     the first pass writes every element the second pass reads.  Calls whose
+//     work overlaps on the GPU (two streams, or several host threads) race on
+//     the array and must be serialised by the caller.
+static constexpr long long kC2sScratchDoubles = 4ll << 20;
+static __device__ __align__(256) double g_c2s_scratch[kC2sScratchDoubles];
+
+static int c2s_scratch_address(double **out)
+{
+    static double *addr[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        set_error("ccsd_b200_cart2sph_s2kl_noalloc: no current CUDA device");
+        return CCSD_B200_ERR_LAUNCH;
+    }
+    if (!addr[dev]) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_c2s_scratch);
+        if (e != cudaSuccess || !p) {
+            set_error("ccsd_b200_cart2sph_s2kl_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+            return CCSD_B200_ERR_LAUNCH;
+        }
+        addr[dev] = static_cast<double *>(p);
+    }
+    *out = addr[dev];
+    return CCSD_B200_OK;
+}
+
+extern "C" int ccsd_b200_cart2sph_s2kl_noalloc(const double *cart, double *out, int ncomp, int nfc, int naoc,
+                                               int nfs, int naos, const int32_t *ptr_i, const int32_t *idx_i,
+                                               const double *val_i, const int32_t *ptr, const int32_t *idx,
+                                               const double *val, void *stream)
+{
+    if (!cart || !out || ncomp <= 0 || nfc <= 0 || naoc <= 0 || nfs <= 0 || naos <= 0 || !ptr_i || !idx_i ||
+        !val_i || !ptr || !idx || !val) {
+        set_error("ccsd_b200_cart2sph_s2kl_noalloc: invalid argument");
+        return CCSD_B200_ERR_ARG;
+    }
+    const long long npc = (long long)naoc * (naoc + 1) / 2;
+    const long long rows = (long long)ncomp * nfs * naos;
+    if (rows > kC2sScratchDoubles || npc > kC2sScratchDoubles / rows) {
+        set_error("ccsd_b200_cart2sph_s2kl_noalloc: the block needs %lld doubles of scratch, the built-in "
+                  "buffer holds %lld (32 MiB); split the i-shell range or use ccsd_b200_cart2sph_s2kl",
+                  rows * npc, kC2sScratchDoubles);
+        return CCSD_B200_ERR_ARG;
+    }
+    double *tmp = nullptr;
+    int rc = c2s_scratch_address(&tmp);
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    const int bs = 256;
+    const long long gmax = (long long)num_sms() * 32;
+    long long g1 = (rows * npc + bs - 1) / bs;
+    if (g1 > gmax) g1 = gmax;
+    c2s_ij_kernel<<<(int)g1, bs, 0, st>>>(cart, tmp, ncomp, nfc, naoc, npc, nfs, naos, ptr_i, idx_i, val_i, ptr,
+                                          idx, val);
+    if ((rc = check_launch("c2s_ij_kernel (no-alloc)"))) return rc;
+    long long g2 = (rows * ((long long)naos * (naos + 1) / 2) + bs - 1) / bs;
+    if (g2 > gmax) g2 = gmax;
+    c2s_kl_kernel<<<(int)g2, bs, 0, st>>>(tmp, out, rows, npc, naos, ptr, idx, val);
+    return check_launch("c2s_kl_kernel (no-alloc)");
+}

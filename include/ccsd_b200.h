@@ -81,6 +81,25 @@ int ccsd_b200_cart2sph_s2kl(const double *cart, double *tmp, double *out, int nc
                             const double *val, void *stream);
 
 /*
+ * ccsd_b200_cart2sph_s2kl without the caller's scratch buffer.  No counterpart
+ * in the reference: it exists for callers that cannot allocate device
+ * memory -- applications that hand this library a device they already manage
+ * with their own pool, or that forbid allocation while a step runs because
+ * cudaMalloc can synchronise the device.  The transform's intermediate
+ * (ncomp * nfs * naos * naoc(naoc+1)/2 doubles) lives in a fixed 32 MiB device
+ * array inside the library, reserved on every GPU that loads it until the
+ * process exits.  Larger blocks are rejected with CCSD_B200_ERR_ARG and a
+ * message giving both sizes.  The first call on a device looks up the array's
+ * address (cudaGetSymbolAddress) and must come before any stream capture.
+ * All calls share the array, so calls that overlap on the GPU race and must
+ * be serialised by the caller.  Allocates nothing; arguments and result as in
+ * ccsd_b200_cart2sph_s2kl.
+ */
+int ccsd_b200_cart2sph_s2kl_noalloc(const double *cart, double *out, int ncomp, int nfc, int naoc, int nfs,
+                                    int naos, const int32_t *ptr_i, const int32_t *idx_i, const double *val_i,
+                                    const int32_t *ptr, const int32_t *idx, const double *val, void *stream);
+
+/*
  * FP64 FMA throughput probe: `blocks` x 256 threads, each running 8
  * independent FMA chains for `iters` iterations (2*8*iters*256*blocks FLOPs).
  * `out` needs blocks*256 doubles (written only in a practically unreachable
