@@ -25,6 +25,7 @@ SIGNATURES = {
     "ccsd_b200_cart2sph_s2kl": (_c_int, [_vp, _vp, _vp, _c_int, _c_int, _c_int, _c_int, _c_int,
                                          _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "ccsd_b200_fp64_fma_probe": (_c_int, [_vp, _c_int, _c_int, _vp]),
+    "ccsd_b200_int1e_cart": (_c_int, [_c_int, _vp, _c_int, _vp, _c_int, _vp, _vp, _c_int, _c_int, _vp, _vp]),
     "ccsd_b200_cart2sph_s2kl_noalloc": (_c_int, [_vp, _vp, _c_int, _c_int, _c_int, _c_int, _c_int,
                                                  _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "ccsd_b200_split_pack": (_c_int, [_c_int, _vp, _vp, _vp, _c_dbl, _vp, _vp, _vp, _c_dbl, _c_int, _c_int,

@@ -100,6 +100,19 @@ int ccsd_b200_cart2sph_s2kl_noalloc(const double *cart, double *out, int ncomp, 
                                     const int32_t *ptr, const int32_t *idx, const double *val, void *stream);
 
 /*
+ * One-electron integrals over DECONTRACTED Cartesian shells, full matrix
+ * out[comp][i][j] (nao = ao_loc[nbas]):
+ *   op 0 overlap, 1 kinetic, 2 nuclear attraction sum_C -Z_C/|r-C|,
+ *   3 1/|r - R_origin| (origin_atom), and 4..7 the same with d/dr on the
+ *   first function (3 components x, y, z).
+ * Replaces libcint's int1e_ovlp/kin/nuc/rinv and int1e_ipovlp/ipkin/ipnuc/iprinv,
+ * which the reference reaches through PySCF's hcore_generator and get_ovlp
+ * (ref: ccsd_gpu/gpu_ccsd_grad.py:554-584).
+ */
+int ccsd_b200_int1e_cart(int op, const int32_t *atm, int natm, const int32_t *bas, int nbas, const double *env,
+                         const int32_t *ao_loc, int lmax, int origin_atom, double *out, void *stream);
+
+/*
  * FP64 FMA throughput probe: `blocks` x 256 threads, each running 8
  * independent FMA chains for `iters` iterations (2*8*iters*256*blocks FLOPs).
  * `out` needs blocks*256 doubles (written only in a practically unreachable
