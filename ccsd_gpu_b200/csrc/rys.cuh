@@ -17,7 +17,7 @@ namespace cb {
 
 // nodes u[0..n-1] ascending, weights w[0..n-1]; any x (NaN goes to the limit branch,
 // the interval index is clamped, so no table access is ever out of range)
-__device__ __noinline__ void rys_roots(int n, double x, double *__restrict__ u,
+static __device__ __noinline__ void rys_roots(int n, double x, double *__restrict__ u,
                                           double *__restrict__ w)
 {
     const double xmax = 40.0 + 5.0 * n;
