@@ -1,0 +1,213 @@
+"""Closed-shell CCSD on the GPU: AO->MO transform, T-amplitude solve, and the
+hooks the gradient needs (a PySCF-like CCSD object).
+
+The reference obtains T amplitudes from gpu4pyscf or PySCF
+(examples/h2o_ccsd_grad.py:128-147); here the RCCSD amplitude equations (the
+form of PySCF's rccsd.update_amps / rintermediates) run through the same
+contraction engine as the Lambda solver, so ``precision`` ("fp64", "tf32x3",
+"bf16x3") applies to both.  Energies, norms, denominators and DIIS are FP64.
+Wvvvv is never formed: its ovvv*t1 parts are folded into o^3 v intermediates
+and the bare (ac|bd) term is one contraction with tau.
+"""
+from types import SimpleNamespace
+
+import numpy as np
+import torch
+
+from . import _native
+from .contract import check_status, contract
+from .gpu_ccsd_lambda import DIIS, DeviceEris, amplitude_norm_sq, solve_lambda_gpu
+
+
+def ao2mo_gpu(mf, mo_coeff=None):
+    """Chemist-notation MO blocks (PySCF ``_ChemistsERIs`` layout) on the GPU, FP64."""
+    C = torch.as_tensor(mf.mo_coeff if mo_coeff is None else mo_coeff, dtype=torch.float64,
+                        device=mf.eri.device)
+    nocc = int((np.asarray(mf.mo_occ) > 0).sum())
+    g = torch.einsum("pqrs,pi->iqrs", mf.eri, C)
+    g = torch.einsum("iqrs,qj->ijrs", g, C)
+    g = torch.einsum("ijrs,rk->ijks", g, C)
+    g = torch.einsum("ijks,sl->ijkl", g, C)
+    dm = 2 * C[:, :nocc] @ C[:, :nocc].T
+    fock = C.T @ (mf.get_hcore() + mf.get_veff(dm=dm)) @ C
+    o, v = slice(0, nocc), slice(nocc, C.shape[1])
+    e = SimpleNamespace(fock=fock, mo_energy=torch.diagonal(fock).clone(), oooo=g[o, o, o, o].contiguous(),
+                        ovoo=g[o, v, o, o].contiguous(), ovvo=g[o, v, v, o].contiguous(),
+                        oovv=g[o, o, v, v].contiguous(), ovov=g[o, v, o, v].contiguous(),
+                        ovvv=g[o, v, v, v].contiguous(), vvvv=g[v, v, v, v].contiguous())
+    del g
+    return DeviceEris(e)
+
+
+def _E(mode):
+    def E(spec, a, b, out=None, alpha=1.0, beta=0.0):
+        return contract(spec, a, b, out=out, alpha=alpha, beta=beta, mode=mode)
+    return E
+
+
+def update_amps_gpu(t1, t2, eris, mode="tf32x3", level_shift=0.0):
+    """One Jacobi step of the RCCSD amplitude equations; returns (t1new, t2new)."""
+    E = _E(mode)
+    nocc, nvir = t1.shape
+    fock = eris.fock
+    foo, fov, fvv = fock[:nocc, :nocc], fock[:nocc, nocc:], fock[nocc:, nocc:]
+    eo, ev = eris.mo_energy[:nocc], eris.mo_energy[nocc:] + level_shift
+    ovov, ovvv, ovoo, ovvo, oovv, oooo = eris.ovov, eris.ovvv, eris.ovoo, eris.ovvo, eris.oovv, eris.oooo
+    t1t1 = torch.einsum("ic,jd->ijcd", t1, t1)
+    tau = t2 + t1t1
+    Lovov = [(2.0, ovov), (-1.0, ovov.permute(0, 3, 2, 1))]
+    Xovvv = [(2.0, ovvv), (-1.0, ovvv.permute(0, 3, 2, 1))]          # [k,d,a,c]: 2(kd|ac) - (kc|ad)
+    Yovoo = [(2.0, ovoo), (-1.0, ovoo.permute(2, 1, 0, 3))]          # [l,c,k,i]: 2(lc|ki) - (kc|li)
+    Foo = foo + E("kcld,ilcd->ki", Lovov, tau)
+    Fvv = fvv - E("kcld,klad->ac", Lovov, tau)
+    Fov = fov + E("kcld,ld->kc", Lovov, t1)
+    yt1 = E("lcki,lc->ki", Yovoo, t1)
+    xt1 = E("kdac,kd->ac", Xovvv, t1)
+    Loo = Foo + fov @ t1.T + yt1
+    Lvv = Fvv - t1.T @ fov + xt1
+    Foo = Foo - torch.diag(eo)
+    Fvv = Fvv - torch.diag(ev)
+    Loo = Loo - torch.diag(eo)
+    Lvv = Lvv - torch.diag(ev)
+    # T1
+    t1n = (fov - 2 * t1 @ fov.T @ t1 + t1 @ Fvv.T - Foo.T @ t1 + t1 @ Fov.T @ t1 + t1 @ xt1.T - yt1.T @ t1)
+    E("kc,kica->ia", Fov, [(2.0, t2), (-1.0, t2.permute(1, 0, 2, 3))], out=t1n, beta=1.0)
+    E("kcai,kc->ia", ovvo, t1, out=t1n, alpha=2.0, beta=1.0)
+    E("kiac,kc->ia", oovv, t1, out=t1n, alpha=-1.0, beta=1.0)
+    E("kdac,ikcd->ia", Xovvv, t2, out=t1n, beta=1.0)
+    E("lcki,klac->ia", Yovoo, t2, out=t1n, alpha=-1.0, beta=1.0)
+    # T2
+    tmp2 = ovvv.permute(1, 3, 0, 2) - torch.einsum("kibc,ka->abic", oovv, t1)
+    tmp = E("abic,jc->ijab", tmp2, t1)
+    t2n = tmp + tmp.permute(1, 0, 3, 2)
+    tmp2 = E("kcai,jc->akij", ovvo, t1)
+    tmp2 += ovoo.permute(1, 3, 0, 2)
+    tmp = E("akij,kb->ijab", tmp2, t1)
+    t2n -= tmp + tmp.permute(1, 0, 3, 2)
+    t2n += ovov.permute(0, 2, 1, 3)
+    Woooo = E("lcki,jc->klij", ovoo, t1)
+    E("kclj,ic->klij", ovoo, t1, out=Woooo, beta=1.0)
+    E("kcld,ijcd->klij", ovov, tau, out=Woooo, beta=1.0)
+    Woooo += oooo.permute(0, 2, 1, 3)
+    E("klij,klab->ijab", Woooo, tau, out=t2n, beta=1.0)
+    # Wvvvv . tau without forming Wvvvv
+    E("acbd,ijcd->ijab", eris.vvvv, tau, out=t2n, beta=1.0)
+    Zt = E("kdac,ijcd->ijka", ovvv, tau)
+    tmp = E("ijka,kb->ijab", Zt, t1)
+    t2n -= tmp + tmp.permute(1, 0, 3, 2)
+    t1t1b = torch.einsum("id,la->ilda", t1, t1)
+    half_t2_t1t1 = [(0.5, t2), (1.0, t1t1b)]
+    Wvoov = ovvo.permute(2, 0, 3, 1).contiguous()
+    E("kcad,id->akic", ovvv, t1, out=Wvoov, beta=1.0)
+    E("kcli,la->akic", ovoo, t1, out=Wvoov, alpha=-1.0, beta=1.0)
+    E("ldkc,ilda->akic", ovov, half_t2_t1t1, out=Wvoov, alpha=-1.0, beta=1.0)
+    E("ldkc,ilad->akic", [(1.0, ovov), (-0.5, ovov.permute(0, 3, 2, 1))], t2, out=Wvoov, beta=1.0)
+    Wvovo = oovv.permute(2, 0, 3, 1).contiguous()
+    E("kdac,id->akci", ovvv, t1, out=Wvovo, beta=1.0)
+    E("lcki,la->akci", ovoo, t1, out=Wvovo, alpha=-1.0, beta=1.0)
+    E("lckd,ilda->akci", ovov, half_t2_t1t1, out=Wvovo, alpha=-1.0, beta=1.0)
+    tmp = E("ac,ijcb->ijab", Lvv, t2)
+    t2n += tmp + tmp.permute(1, 0, 3, 2)
+    tmp = E("ki,kjab->ijab", Loo, t2)
+    t2n -= tmp + tmp.permute(1, 0, 3, 2)
+    tmp = E("akic,kjcb->ijab", [(2.0, Wvoov), (-1.0, Wvovo.permute(0, 1, 3, 2))], t2)
+    t2n += tmp + tmp.permute(1, 0, 3, 2)
+    tmp = E("akic,kjbc->ijab", Wvoov, t2)
+    t2n -= tmp + tmp.permute(1, 0, 3, 2)
+    tmp = E("bkci,kjac->ijab", Wvovo, t2)
+    t2n -= tmp + tmp.permute(1, 0, 3, 2)
+    eia = eo[:, None] - ev[None, :]
+    return t1n / eia, t2n / (eia[:, None, :, None] + eia[None, :, None, :])
+
+
+def energy_gpu(t1, t2, eris):
+    nocc = t1.shape[0]
+    tau = t2 + torch.einsum("ia,jb->ijab", t1, t1)
+    ov = eris.ovov
+    return float(2 * (eris.fock[:nocc, nocc:] * t1).sum() + 2 * torch.einsum("ijab,iajb->", tau, ov)
+                 - torch.einsum("ijab,ibja->", tau, ov))
+
+
+class CCSD:
+    """PySCF-like closed-shell CCSD on the GPU (frozen core off)."""
+
+    def __init__(self, mf, precision="tf32x3"):
+        _native.require_cuda()
+        self._scf = mf
+        self.mol = mf.mol
+        self.mo_coeff = mf.mo_coeff
+        self.mo_occ = mf.mo_occ
+        self.mo_energy = mf.mo_energy
+        self.precision = precision
+        self.max_cycle = 100
+        self.conv_tol = 1e-9
+        self.conv_tol_normt = 1e-7
+        self.t_polish = True
+        self.lambda_polish = True
+        self.diis_space = 8
+        self.level_shift = 0.0
+        self.verbose = 0
+        self.t1 = self.t2 = self.l1 = self.l2 = None
+        self.converged = self.converged_lambda = False
+        self._eris = None
+
+    @property
+    def nocc(self):
+        return int((np.asarray(self.mo_occ) > 0).sum())
+
+    def ao2mo(self, mo_coeff=None):
+        if self._eris is None or mo_coeff is not None:
+            self._eris = ao2mo_gpu(self._scf, mo_coeff)
+        return self._eris
+
+    def kernel(self, t1=None, t2=None, eris=None):
+        eris = self.ao2mo() if eris is None else DeviceEris.wrap(eris)
+        nocc = self.nocc
+        eo, ev = eris.mo_energy[:nocc], eris.mo_energy[nocc:]
+        eia = eo[:, None] - ev[None, :]
+        d2 = eia[:, None, :, None] + eia[None, :, None, :]
+        t1 = eris.fock[:nocc, nocc:] / eia if t1 is None else torch.as_tensor(t1, device=eia.device)
+        t2 = eris.ovov.permute(0, 2, 1, 3) / d2 if t2 is None else torch.as_tensor(t2, device=eia.device)
+        adiis = DIIS(self.diis_space)
+        e_old = energy_gpu(t1, t2, eris)
+        nov = t1.numel()
+        self.converged = False
+        # split precision down to its ~1e-6 noise floor, then FP64 iterations
+        # (mixed-precision iterative refinement; ``t_polish = False`` skips them)
+        mode = self.precision
+        tol_n = self.conv_tol_normt if mode == "fp64" else max(self.conv_tol_normt, 1e-6)
+        self._t_history = []
+        for it in range(self.max_cycle):
+            t1n, t2n = update_amps_gpu(t1, t2, eris, mode, self.level_shift)
+            normt = float(torch.sqrt(amplitude_norm_sq(t1n - t1, t2n - t2)))
+            self._t_history.append((mode, normt))
+            x = adiis.update(torch.cat([t1n.reshape(-1), t2n.reshape(-1)]),
+                             torch.cat([(t1n - t1).reshape(-1), (t2n - t2).reshape(-1)]))
+            t1, t2 = x[:nov].reshape(t1.shape), x[nov:].reshape(t2.shape)
+            e = energy_gpu(t1, t2, eris)
+            if normt < tol_n and abs(e - e_old) < self.conv_tol:
+                if mode != "fp64" and self.t_polish and self.conv_tol_normt < tol_n:
+                    mode, tol_n = "fp64", self.conv_tol_normt
+                    adiis = DIIS(self.diis_space)
+                    e_old = e
+                    continue
+                self.converged = True
+                break
+            e_old = e
+        check_status()
+        self.e_corr = e
+        self._t1g, self._t2g = t1, t2
+        self.t1, self.t2 = t1.cpu().numpy(), t2.cpu().numpy()
+        return self.e_corr, self.t1, self.t2
+
+    @property
+    def e_tot(self):
+        return self._scf.e_tot + self.e_corr
+
+    def solve_lambda(self, t1=None, t2=None, l1=None, l2=None, eris=None):
+        return solve_lambda_gpu(self, t1, t2, l1, l2, eris=self.ao2mo() if eris is None else eris,
+                                mode=self.precision)
+
+    def nuc_grad_method(self):
+        from .gpu_ccsd_grad import Gradients
+        return Gradients(self)

@@ -256,9 +256,19 @@ class DIIS:
         return (c[:, None] * torch.stack(self.xs)).sum(0)
 
 
+MIXED_FLOOR = 1e-6     # update norm below which split-precision iterations stop helping
+
+
 def kernel_gpu(mycc, eris=None, t1=None, t2=None, l1=None, l2=None, max_cycle=None, tol=None, verbose=None,
-               use_cpu_vvvv=True, mode=None):
-    """Iterate to ||delta lambda|| < tol (ref: ccsd_gpu/gpu_ccsd_lambda.py:340-408)."""
+               use_cpu_vvvv=True, mode=None, polish=None):
+    """Iterate to ||delta lambda|| < tol (ref: ccsd_gpu/gpu_ccsd_lambda.py:340-408).
+
+    In a split-precision mode the iterations run in that mode down to
+    max(tol, 1e-6); if ``tol`` is tighter and ``polish`` (default: the CC
+    object's ``lambda_polish``, else True) is set, the intermediates are
+    rebuilt in FP64 and FP64 iterations finish the solve (mixed-precision
+    iterative refinement: the fixed point is the FP64 one).
+    """
     _native.require_cuda()
     if eris is None:
         eris = mycc.ao2mo()
@@ -270,24 +280,34 @@ def kernel_gpu(mycc, eris=None, t1=None, t2=None, l1=None, l2=None, max_cycle=No
     max_cycle = getattr(mycc, "max_cycle", 50) if max_cycle is None else max_cycle
     tol = getattr(mycc, "conv_tol_normt", 1e-5) if tol is None else tol
     mode = _mode_of(mycc, mode)
+    polish = getattr(mycc, "lambda_polish", True) if polish is None else polish
     t1g, t2g, l1g, l2g = _t(t1), _t(t2), _t(l1), _t(l2)
-    imds = make_intermediates_gpu(mycc, t1g, t2g, eris, mode)
-    adiis = DIIS(getattr(mycc, "diis_space", 6)) if getattr(mycc, "diis", True) else None
+    cur_mode = mode
+    cur_tol = tol if mode == "fp64" else max(tol, MIXED_FLOOR)
+    imds = make_intermediates_gpu(mycc, t1g, t2g, eris, cur_mode)
+    space = getattr(mycc, "diis_space", 6)
+    use_diis = getattr(mycc, "diis", True)
+    adiis = DIIS(space) if use_diis else None
     nov = l1g.numel()
     conv = False
     history = []
     for istep in range(max_cycle):
-        l1n, l2n = update_lambda_gpu(mycc, t1g, t2g, l1g, l2g, eris, imds, mode=mode)
+        l1n, l2n = update_lambda_gpu(mycc, t1g, t2g, l1g, l2g, eris, imds, mode=cur_mode)
         normt = float(torch.sqrt(amplitude_norm_sq(l1n - l1g, l2n - l2g)))
-        history.append(normt)
+        history.append((cur_mode, normt))
         if adiis is not None:
             x = torch.cat([l1n.reshape(-1), l2n.reshape(-1)])
             e = torch.cat([(l1n - l1g).reshape(-1), (l2n - l2g).reshape(-1)])
             x = adiis.update(x, e)
             l1n, l2n = x[:nov].reshape(l1g.shape), x[nov:].reshape(l2g.shape)
         l1g, l2g = l1n, l2n
-        if normt < tol:
-            conv = True
+        if normt < cur_tol:
+            if cur_mode != "fp64" and polish and tol < cur_tol:
+                cur_mode, cur_tol = "fp64", tol
+                imds = make_intermediates_gpu(mycc, t1g, t2g, eris, "fp64")
+                adiis = DIIS(space) if use_diis else None
+                continue
+            conv = normt < tol or (cur_mode != "fp64" and not polish)
             break
     check_status()
     mycc._lambda_history = history

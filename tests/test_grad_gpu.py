@@ -1,0 +1,105 @@
+"""GPU chemistry chain against the oracle: RHF, CCSD, RDMs, the full CCSD
+gradient (oracle pinned to central finite differences) and the autograd path."""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import cc_oracle as C
+from oracle import scf_cc_oracle as Q
+from tests.conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+H2O = "O 0 0 0; H 0 -0.757 0.587; H 0.05 0.757 0.587"
+
+
+@pytest.fixture(scope="module")
+def h2o_oracle():
+    from ccsd_gpu_b200.gto import M
+    mol = M(atom=H2O, basis="cc-pvdz")
+    mf, eris, etot, t1, t2 = Q.ccsd_total(mol)
+    l1, l2 = Q.lambda_solve(t1, t2, eris)
+    g = Q.grad_elec(mf, t1, t2, l1, l2) + mol.grad_nuc()
+    return dict(mol=mol, mf=mf, etot=etot, t1=t1, t2=t2, l1=l1, l2=l2, grad=g)
+
+
+def test_rhf_energy_matches_oracle(h2o_oracle):
+    from ccsd_gpu_b200.scf import RHF
+    mf = RHF(h2o_oracle["mol"]).run()
+    assert mf.converged
+    assert abs(mf.e_tot - h2o_oracle["mf"].e_tot) < 1e-9
+
+
+@pytest.mark.parametrize("mode,tol", [("fp64", 1e-9), ("tf32x3", 1e-7)])
+def test_ccsd_energy_matches_oracle(h2o_oracle, mode, tol):
+    from ccsd_gpu_b200.ccsd import CCSD
+    from ccsd_gpu_b200.scf import RHF
+    cc = CCSD(RHF(h2o_oracle["mol"]).run(), precision=mode)
+    cc.kernel()
+    assert cc.converged
+    assert abs(cc.e_tot - h2o_oracle["etot"]) < tol
+
+
+@pytest.mark.parametrize("mode,tol", [("fp64", 1e-12), ("tf32x3", 5e-6)])
+def test_rdm_intermediates_match_reference_golden(mode, tol):
+    from types import SimpleNamespace
+    from ccsd_gpu_b200 import gpu_ccsd_grad as G
+    d = dict(np.load(os.path.join(GOLDEN, "cc_small.npz")))
+    cc = SimpleNamespace(precision=mode)
+    args = (d["t1"], d["t2"], d["l1"], d["l2"])
+    rel = lambda a, b: float(np.abs(a.cpu().numpy() - b).max() / np.abs(b).max())   # noqa: E731
+    for k, a in zip(("doo", "dov", "dvo", "dvv"), G._gamma1_intermediates_gpu(cc, *args)):
+        assert rel(a, d[k]) < tol, k
+    d2 = G._gamma2_intermediates_gpu(cc, *args)
+    for k, a in zip(("dovov", "dvvvv", "doooo", "doovv", "dovvo", "dvvov", "dovvv", "dooov"), d2):
+        if a is not None:
+            assert rel(a, d[k]) < tol, k
+    assert rel(G._rdm2_mo2ao_gpu(cc, d2, d["mo_coeff"]), d["dm2_tril"]) < tol
+
+
+@pytest.mark.parametrize("mode,polish,tol", [("fp64", True, 1e-7), ("tf32x3", True, 1e-6),
+                                              ("tf32x3", False, 1e-6), ("bf16x3", True, 1e-6)])
+def test_ccsd_gradient_matches_oracle(h2o_oracle, mode, polish, tol):
+    """Mixed precision with and without the FP64 polish of the Lambda solve,
+    against the FP64 oracle: the north-star bar is max|dg| <= 1e-6 Eh/bohr."""
+    from ccsd_gpu_b200.ccsd import CCSD
+    from ccsd_gpu_b200.scf import RHF
+    cc = CCSD(RHF(h2o_oracle["mol"]).run(), precision=mode)
+    cc.kernel()
+    cc.conv_tol_normt = 1e-9
+    cc.lambda_polish = polish
+    cc.solve_lambda()
+    assert cc.converged_lambda
+    g = cc.nuc_grad_method().kernel()
+    assert np.abs(g - h2o_oracle["grad"]).max() < tol
+    assert np.abs(g.sum(0)).max() < 1e-8
+
+
+def test_compute_ml_ccsd_forces_gpu_with_oracle_amplitudes(h2o_oracle):
+    from ccsd_gpu_b200.gpu_ccsd_grad import compute_ml_ccsd_forces_gpu
+    from ccsd_gpu_b200.scf import RHF
+    o = h2o_oracle
+    mf = RHF(o["mol"]).run()
+    # the amplitudes belong to the oracle's orbitals (MO signs are arbitrary per SCF run)
+    mf.mo_coeff, mf.mo_energy = o["mf"].mo_coeff, o["mf"].mo_energy
+    g = compute_ml_ccsd_forces_gpu(mf, o["t1"], o["t2"], o["l1"], o["l2"], precision="fp64")
+    assert np.abs(g - o["grad"]).max() < 1e-7
+
+
+def test_autograd_energy_backward_and_finite_difference():
+    from ccsd_gpu_b200.gpu_ccsd_grad import CCSDEnergy
+    from ccsd_gpu_b200.gto import M
+    mol = M(atom=H2O, basis="sto-3g")
+    x = torch.tensor(mol.atom_coords(), dtype=torch.float64, device="cuda", requires_grad=True)
+    e = CCSDEnergy.apply(x, mol, "fp64")
+    e.backward()
+    h = 1e-3
+    for a, c in [(0, 2), (2, 0)]:
+        xs = []
+        for s in (1, -1):
+            y = x.detach().clone()
+            y[a, c] += s * h
+            xs.append(float(CCSDEnergy.apply(y, mol, "fp64")))
+        assert abs((xs[0] - xs[1]) / (2 * h) - float(x.grad[a, c])) < 5e-7
