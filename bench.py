@@ -1,16 +1,27 @@
 #!/usr/bin/env python
-"""ERI microbenchmark on B200: FP64 int2e_ip1 (and int2e) over synthetic shells.
+"""Benchmarks of the CCSD-gradient hot path on B200.
 
-Workload: 4096 shells, l in {0,1,2} (s:p:d = 4:3:2), 1-6 primitives,
-exponents log-uniform in [0.05, 1e4], centres in a 12-bohr cube, seed 0; a
-seeded uniform sample of unique shell quartets passing a 1e-12 Schwarz
-screen, sorted by L-class.  One step = int2e_ip1 of every sampled quartet,
-consumed in-kernel (two checksums per quartet and component).
+Default workload ``eri`` -- ERI microbenchmark, FP64 int2e_ip1 (and int2e)
+over synthetic shells: 4096 shells, l in {0,1,2} (s:p:d = 4:3:2), 1-6
+primitives, exponents log-uniform in [0.05, 1e4], centres in a 12-bohr cube,
+seed 0; a seeded uniform sample of unique shell quartets passing a 1e-12
+Schwarz screen, sorted by L-class.  One step = int2e_ip1 of every sampled
+quartet, consumed in-kernel (two checksums per quartet and component).
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Other workloads (``--workload``):
+  lambda  Lambda/2-RDM contractions on a synthetic CCSD state (nocc 24,
+          nvir 216): intermediates + 20 Jacobi Lambda updates + the 1- and
+          2-particle density intermediates, once in FP64 (cuBLAS) and once in
+          the split-precision tensor-core mode; errors of l1, l2 and the
+          2-RDM blocks against the FP64 run.
+  gemm    the split-precision tcgen05 GEMM alone (4096^3 and the vvvv-ladder
+          shape 576 x 46656 x 46656) against cuBLAS DGEMM.
 
-Multi-GPU (torchrun): every rank draws its own sample (weak scaling, no
-data-path collective); time = max over ranks.
+  python bench.py [--workload eri|lambda|gemm] [--gpus N] [--steps K] [--warmup W]
+                  [--impl ours|reference]
+
+Multi-GPU (torchrun): every rank runs its own copy of the workload (weak
+scaling, no data-path collective); time = max over ranks.
 """
 import argparse
 import json
@@ -31,13 +42,24 @@ NSHELL = 4096
 
 def parse():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", choices=["eri", "lambda", "gemm"], default="eri")
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=None)
+    ap.add_argument("--warmup", type=int, default=None)
+    ap.add_argument("--mode", default="tf32x3", help="split-precision mode of the lambda/gemm workloads")
+    ap.add_argument("--nocc", type=int, default=24)
+    ap.add_argument("--nvir", type=int, default=216)
+    ap.add_argument("--iters", type=int, default=20, help="Lambda iterations per lambda-workload step")
+    ap.add_argument("--gemm-shapes", choices=["all", "square"], default="all",
+                    help="gemm workload: both shapes, or only the 4096^3 one (small, for profiling)")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--quartets", type=int, default=1 << 18, help="sampled quartets per rank per step")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU-baseline sample budget")
-    return ap.parse_args()
+    args = ap.parse_args()
+    dflt = {"eri": (10, 3), "lambda": (3, 3), "gemm": (10, 3)}[args.workload]
+    args.steps = dflt[0] if args.steps is None else args.steps
+    args.warmup = dflt[1] if args.warmup is None else args.warmup
+    return args
 
 
 def dist_setup():
@@ -173,11 +195,178 @@ def run_reference_arm(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
+def _events_timed(fn, steps, barrier, flush=None):
+    """Per-step CUDA-event times (ms) on the current stream, plus the region time."""
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    barrier()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for a, b in evs:
+        if flush is not None:
+            flush.fill_(1)
+        a.record()
+        fn()
+        b.record()
+    t1.record()
+    barrier()
+    return np.array([a.elapsed_time(b) for a, b in evs]), t0.elapsed_time(t1)
+
+
+def _maxr(x, ws, dev):
+    if ws == 1:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _tensor_peak():
+    """TF32 dense peak used as the tensor roofline of the split-precision GEMMs:
+    half of the measured bf16 GEMM peak (B200: TF32 runs at half the BF16 rate)."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            pk = json.load(f)
+        return pk["bf16_tflops"] / 2, "half of the measured bf16 burst peak (%.1f TF/s)" % pk["bf16_tflops"]
+    except (OSError, KeyError, ValueError):
+        return 1590.0 / 2, "half of the 1.59 PF/s bf16 fallback"
+
+
+def run_gemm(args, ws, rank, local):
+    """Split-precision tcgen05 GEMM vs cuBLAS DGEMM (one launch = one GEMM)."""
+    from ccsd_gpu_b200.contract import STATS, check_status, contract, mark_constant, reset_stats
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    barrier = (lambda: (torch.distributed.barrier(), torch.cuda.synchronize(dev))) if ws > 1 else \
+        (lambda: torch.cuda.synchronize(dev))
+    g = torch.Generator(device=dev).manual_seed(rank)
+    peak, peak_src = _tensor_peak()
+    res = {}
+    shapes = [("square_4096", 4096, 4096, 4096), ("vvvv_ladder_o24_v216", 576, 46656, 46656)]
+    for name, M, N, K in shapes[:1 if args.gemm_shapes == "square" else 2]:
+        a = torch.randn(M, K, dtype=torch.float64, device=dev, generator=g)
+        b = torch.randn(N, K, dtype=torch.float64, device=dev, generator=g)
+        mark_constant(a, b)                      # packed once; the timed region is the GEMM launch
+        out = torch.empty(M, N, dtype=torch.float64, device=dev)
+        run = lambda: contract("mk,nk->mn", a, b, out=out, mode=args.mode)   # noqa: E731
+        for _ in range(args.warmup):
+            run()
+        reset_stats()
+        with ClockSampler(dev) as clk:
+            ks, _ = _events_timed(run, args.steps, barrier)
+        launches = STATS["launches"]
+        check_status(dev)
+        ms = _maxr(float(ks.mean()), ws, dev)
+        ref = a @ b.T
+        err = float((out - ref).abs().max() / ref.abs().max())
+        dg = lambda: torch.mm(a, b.T, out=ref)   # noqa: E731
+        dg()
+        kd, _ = _events_timed(dg, max(3, args.steps // 2), barrier)
+        ms_d = _maxr(float(kd.mean()), ws, dev)
+        fl = 2.0 * M * N * K
+        res[name] = {"ms": ms, "fp64_equiv_tflops": fl / ms / 1e9, "tensor_tflops": 3 * fl / ms / 1e9,
+                     "dgemm_ms": ms_d, "dgemm_tflops": fl / ms_d / 1e9, "speedup_vs_dgemm": ms_d / ms,
+                     "max_rel_err_vs_dgemm": err, "launches_timed": launches, "clocks": clk.summary()}
+        del a, b, out, ref
+        torch.cuda.empty_cache()
+    head = res[list(res)[-1]]
+    line = {"metric": "split-precision GEMM FP64-equivalent TFLOP/s (%s, vvvv-ladder shape)" % args.mode,
+            "value": head["fp64_equiv_tflops"] * ws, "unit": "TFLOP/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": head["ms"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": args.mode, "data": "synthetic",
+            "config": {"workload": "tc_split_gemm", "headline_shape": list(res)[-1], "shapes": res,
+                       "l2": "operands larger than L2 (vvvv shape: 17.4 GB B operand)",
+                       "parallelism": "dp%d" % ws if ws > 1 else "single"},
+            "roofline": {"bound": "tensor", "achieved": head["tensor_tflops"], "peak": peak, "unit": "TFLOP/s",
+                         "frac": head["tensor_tflops"] / peak, "traffic": None,
+                         "peak_source": peak_src, "flops": "3 TF32 products x 2 M N K per GEMM"},
+            "gpu_launches": head["launches_timed"], "clocks": head["clocks"], "cpu_baseline": None,
+            "e2e": None}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def _rel(a, b):
+    d = float((a - b).abs().max())
+    m = float(b.abs().max())
+    return d / m if m > 0 else d
+
+
+def run_lambda(args, ws, rank, local):
+    """Lambda/2-RDM contraction bench on a synthetic CCSD state."""
+    from types import SimpleNamespace
+    from ccsd_gpu_b200 import workloads
+    from ccsd_gpu_b200.contract import STATS, check_status, reset_stats
+    from ccsd_gpu_b200.gpu_ccsd_grad import _gamma1_intermediates_gpu, _gamma2_intermediates_gpu
+    from ccsd_gpu_b200.gpu_ccsd_lambda import DeviceEris, make_intermediates_gpu, update_lambda_gpu
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    barrier = (lambda: (torch.distributed.barrier(), torch.cuda.synchronize(dev))) if ws > 1 else \
+        (lambda: torch.cuda.synchronize(dev))
+    eris, t1, t2 = workloads.lambda_bench_state(args.nocc, args.nvir, seed=rank, device=dev)
+    deris = DeviceEris(eris, dev)
+    del eris
+    keep = {}
+
+    def solve(mode):
+        cc = SimpleNamespace(level_shift=0.0, precision=mode)
+        imds = make_intermediates_gpu(cc, t1, t2, deris, mode)
+        l1, l2 = t1, t2
+        for _ in range(args.iters):
+            l1, l2 = update_lambda_gpu(cc, t1, t2, l1, l2, deris, imds, mode=mode)
+        d1 = _gamma1_intermediates_gpu(cc, t1, t2, l1, l2)
+        d2 = _gamma2_intermediates_gpu(cc, t1, t2, l1, l2)
+        keep[mode] = (l1, l2, d1, d2)
+
+    out = {}
+    for mode in ("fp64", args.mode):
+        keep.pop(mode, None)
+        for _ in range(args.warmup):
+            solve(mode)
+        reset_stats()
+        with ClockSampler(dev) as clk:
+            ks, region = _events_timed(lambda: solve(mode), args.steps, barrier)
+        check_status(dev)
+        out[mode] = {"s_per_run": _maxr(float(ks.mean()), ws, dev) * 1e-3, "flops": STATS["flops"] / args.steps,
+                     "launches": STATS["launches"] // args.steps, "clocks": clk.summary()}
+        if mode != "fp64":
+            ref, got = keep["fp64"], keep[mode]
+            d2e = max(_rel(x, y) for x, y in zip(got[3], ref[3]) if x is not None)
+            d1e = max(_rel(x, y) for x, y in zip(got[2], ref[2]))
+            out[mode].update(l1_rel_err=_rel(got[0], ref[0]), l2_rel_err=_rel(got[1], ref[1]),
+                             rdm1_rel_err=d1e, rdm2_rel_err=d2e)
+            del keep["fp64"]
+        torch.cuda.empty_cache()
+    fp, mx = out["fp64"], out[args.mode]
+    peak, peak_src = _tensor_peak()
+    ach = 3 * mx["flops"] / mx["s_per_run"] / 1e12
+    line = {"metric": "Lambda/2-RDM run time (nocc %d, nvir %d, %d Lambda iterations + RDM intermediates), %s vs FP64"
+                      % (args.nocc, args.nvir, args.iters, args.mode),
+            "value": mx["s_per_run"], "unit": "s/run", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": mx["s_per_run"] * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": args.mode, "data": "synthetic",
+            "config": {"workload": "lambda_rdm_o%d_v%d" % (args.nocc, args.nvir), "iterations": args.iters,
+                       "state": "seeded synthetic CCSD state (lambda_bench_state)",
+                       "l2": "operands larger than L2 (vvvv block 17.4 GB)",
+                       "parallelism": "dp%d" % ws if ws > 1 else "single"},
+            "fp64": fp, "mixed": mx, "speedup_vs_fp64": fp["s_per_run"] / mx["s_per_run"],
+            "roofline": {"bound": "tensor", "achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak,
+                         "traffic": None, "peak_source": peak_src,
+                         "flops": "3 TF32 products x counted 2 M N K of every contraction in the run"},
+            "gpu_launches": mx["launches"], "clocks": mx["clocks"], "cpu_baseline": None, "e2e": None}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     ws, rank, local = dist_setup()
     if args.impl == "reference":
         run_reference_arm(args, ws, rank)
+        if ws > 1:
+            torch.distributed.destroy_process_group()
+        return
+    if args.workload != "eri":
+        (run_gemm if args.workload == "gemm" else run_lambda)(args, ws, rank, local)
         if ws > 1:
             torch.distributed.destroy_process_group()
         return

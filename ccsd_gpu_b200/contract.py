@@ -19,6 +19,8 @@ D[m, n] = sum_k A[m, k] B[n, k]:
   * mode "fp64": ``torch.einsum`` in float64 (cuBLAS DGEMM): the plain FP64 GPU
     path the split-precision modes are measured against.
 """
+import weakref
+
 import numpy as np
 import torch
 
@@ -78,6 +80,16 @@ def check_status(device=None):
 
 _off_cache = {}
 
+# running totals, read by benchmarks: algorithmic FLOPs (2 M N K per GEMM, FP64
+# equivalent) and native launches (pack + GEMM) of the split-precision modes;
+# FLOPs of the fp64 mode are counted the same way
+STATS = {"flops": 0, "launches": 0, "gemms": 0}
+
+
+def reset_stats():
+    for k in STATS:
+        STATS[k] = 0
+
 
 def _dev_offsets(key, make, dev):
     t = _off_cache.get((key, dev))
@@ -89,7 +101,68 @@ def _dev_offsets(key, make, dev):
     return t
 
 
+# ---- packed-operand cache ---------------------------------------------------------
+# Operands whose storage was registered with mark_constant() keep their packed
+# hi/lo arrays between calls (the MO integral blocks of the Lambda and CCSD
+# iterations: vvvv alone is nvir^4 values).  The key holds every term's
+# storage, offset, strides, shape, coefficient and torch version counter, so
+# an in-place torch update of a registered tensor misses the cache; entries
+# die with the registered tensor.
+_const = {}                  # storage data_ptr -> weakref to the registered tensor
+_pack_cache = {}             # key -> (hi, lo)
+_PACK_CACHE_BYTES = 64 << 30
+
+
+def mark_constant(*tensors):
+    """Declare tensors read-only for the rest of their life: contractions keep
+    their split/packed forms instead of re-packing them on every call."""
+    for t in tensors:
+        if t is None or not isinstance(t, torch.Tensor) or t.device.type != "cuda":
+            continue
+        ptr = t.untyped_storage().data_ptr()
+        _const[ptr] = weakref.ref(t, lambda _r, ptr=ptr: _forget(ptr))
+
+
+def _forget(ptr):
+    _const.pop(ptr, None)
+    for k in [k for k in _pack_cache if ptr in k[-1]]:
+        del _pack_cache[k]
+
+
+def clear_pack_cache():
+    _pack_cache.clear()
+
+
+def _is_const(t):
+    r = _const.get(t.untyped_storage().data_ptr())
+    return r is not None and r() is not None
+
+
+def _cache_key(terms, sub, rows_idx, k_idx, shape_map, kind, rows_pad, k_pad):
+    if not all(_is_const(t) for _, t in terms):
+        return None
+    desc = tuple((c, t.storage_offset(), tuple(t.stride()), tuple(t.shape), t._version) for c, t in terms)
+    ptrs = tuple(t.untyped_storage().data_ptr() for _, t in terms)
+    return (kind, rows_pad, k_pad, sub, tuple(rows_idx), tuple(k_idx),
+            tuple(shape_map[i] for i in rows_idx + k_idx), desc, ptrs)
+
+
 def _pack(terms, sub, rows_idx, k_idx, shape_map, kind, rows_pad, k_pad, dev, stream):
+    key = _cache_key(terms, sub, rows_idx, k_idx, shape_map, kind, rows_pad, k_pad)
+    if key is not None and key in _pack_cache:
+        return _pack_cache[key]
+    hi, lo = _pack_new(terms, sub, rows_idx, k_idx, shape_map, kind, rows_pad, k_pad, dev, stream)
+    if key is not None:
+        for k in [k for k in _pack_cache if k[:7] == key[:7] and k[-1] == key[-1]]:
+            del _pack_cache[k]        # an older version of the same operand
+        used = sum(h.numel() * 2 for h, _ in _pack_cache.values())
+        if used + 2 * hi.numel() > _PACK_CACHE_BYTES:
+            _pack_cache.clear()
+        _pack_cache[key] = (hi, lo)
+    return hi, lo
+
+
+def _pack_new(terms, sub, rows_idx, k_idx, shape_map, kind, rows_pad, k_pad, dev, stream):
     rows = int(np.prod([shape_map[i] for i in rows_idx])) if rows_idx else 1
     K = int(np.prod([shape_map[i] for i in k_idx])) if k_idx else 1
     esz = 4 if kind == 0 else 2
@@ -107,6 +180,7 @@ def _pack(terms, sub, rows_idx, k_idx, shape_map, kind, rows_pad, k_pad, dev, st
         p2 = (_native.ptr(t2), _native.ptr(o2r), _native.ptr(o2k), c2)
     else:
         p2 = (_native.ptr(None), _native.ptr(None), _native.ptr(None), 0.0)
+    STATS["launches"] += 1
     _native.call("ccsd_b200_split_pack", kind, _native.ptr(t1), _native.ptr(o1r), _native.ptr(o1k), c1, *p2,
                  rows, K, rows_pad, k_pad, _native.ptr(hi), _native.ptr(lo), stream)
     return hi, lo
@@ -131,6 +205,9 @@ def contract(spec, a, b, out=None, alpha=1.0, beta=0.0, mode="tf32x3", stream=No
         out = torch.zeros([shape_map[i] for i in so], dtype=torch.float64, device=dev)
         beta = 0.0
     if mode == "fp64":
+        n_all = int(np.prod(list(shape_map.values())))
+        STATS["flops"] += 2 * n_all * len(ta) * len(tb)
+        STATS["gemms"] += len(ta) * len(tb)
         res = None
         for c1, t1 in ta:
             for c2, t2 in tb:
@@ -178,7 +255,28 @@ def contract(spec, a, b, out=None, alpha=1.0, beta=0.0, mode="tf32x3", stream=No
     key_n = ("on", tuple(n_idx), so, tuple(out.stride()), tuple(shape_map[i] for i in n_idx))
     om = _dev_offsets(key_m, lambda: _offsets(m_idx, so, shape_map, out), dev)
     on = _dev_offsets(key_n, lambda: _offsets(n_idx, so, shape_map, out), dev)
+    ksplit = _ksplit(m_pad, n_pad, k_pad // kal, dev)
+    partial = torch.empty(ksplit * M * N, dtype=torch.float64, device=dev) if ksplit > 1 else None
+    STATS["flops"] += 2 * M * N * K
+    STATS["gemms"] += 1
+    STATS["launches"] += 1 if ksplit == 1 else 2
     _native.call("ccsd_b200_tc_split_gemm", kind, _native.ptr(ahi), _native.ptr(alo), _native.ptr(bhi),
                  _native.ptr(blo), M, N, m_pad, n_pad, k_pad, _native.ptr(out), _native.ptr(om), _native.ptr(on),
-                 float(alpha), float(beta), _native.ptr(_Status.get(dev)), st)
+                 float(alpha), float(beta), ksplit, _native.ptr(partial), _native.ptr(_Status.get(dev)), st)
     return out
+
+
+_sm_count = {}
+_KB_PER_CHUNK = 16        # k blocks per FP32 accumulation chunk in the kernel (512 k)
+
+
+def _ksplit(m_pad, n_pad, kblocks, dev):
+    """Split-K factor: enough CTAs for two waves on the SMs when the output has
+    few 128 x 128 tiles, with at least one 512-k chunk per split."""
+    sms = _sm_count.get(dev)
+    if sms is None:
+        sms = _sm_count[dev] = torch.cuda.get_device_properties(dev).multi_processor_count
+    tiles = (m_pad // _BM) * (n_pad // _BM)
+    if tiles >= sms or kblocks < 2 * _KB_PER_CHUNK:
+        return 1
+    return int(max(1, min(-(-2 * sms // tiles), kblocks // _KB_PER_CHUNK)))

@@ -16,15 +16,20 @@
 // "2 t - t^T" combinations fuse into the pack), splits every value into hi and
 // lo parts and writes K-major, zero-padded [rows_pad x k_pad] arrays for TMA.
 //
-// CTA = 192 threads, one 128 x 128 output tile:
+// CTA = 320 threads, one 128 x 128 output tile:
 //   warp 0      TMA producer (lane 0) into a 3-stage ring of {A_hi, A_lo, B_hi,
 //               B_lo} tiles (128 rows x 128 B, 128 B swizzle); owns TMEM alloc.
 //   warp 1      MMA issuer (lane 0); commits stage releases and chunk-ready.
-//   warps 2..5  drain TMEM (warp w reads lanes 32*(w%4) .. +31) into FP64.
+//   warps 2..9  drain TMEM: warp w reads lanes 32*(w%4) .. +31, columns
+//               64*((w-2)/4) .. +63, and keeps its 32 x 64 block as FP64
+//               running sums in registers across all k chunks; the output is
+//               written once, after the last chunk.
 // Every mbarrier wait is bounded by the global timer (2 s): on expiry the
 // thread records a code in `status` and leaves its loop -- no trap, no
 // unbounded spin.
 #include "common.cuh"
+
+#include <algorithm>
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -38,8 +43,10 @@ static constexpr int TC_STAGES = 3;
 static constexpr int TC_ROWB = 128;                      // bytes per tile row (swizzle span)
 static constexpr int TC_TILE_BYTES = TC_BM * TC_ROWB;    // 16 KiB
 static constexpr int TC_STAGE_BYTES = 4 * TC_TILE_BYTES;
-static constexpr int TC_THREADS = 192;
+static constexpr int TC_DRAIN_WARPS = 8;                // 2 per TMEM lane quadrant
+static constexpr int TC_THREADS = 64 + 32 * TC_DRAIN_WARPS;
 static constexpr int TC_CHUNK_K = 512;                   // k per FP32 accumulation chunk
+static constexpr int TC_GROUP_M = 8;                     // row tiles per raster group
 static constexpr unsigned long long TC_WAIT_NS = 2000000000ull;
 
 enum { KIND_TF32 = 0, KIND_BF16 = 1 };
@@ -169,18 +176,34 @@ template <int KIND>
 __global__ void __launch_bounds__(TC_THREADS, 1) tc_split_gemm_kernel(
     const __grid_constant__ CUtensorMap map_ahi, const __grid_constant__ CUtensorMap map_alo,
     const __grid_constant__ CUtensorMap map_bhi, const __grid_constant__ CUtensorMap map_blo,
-    int M, int N, int kblocks, double *__restrict__ out, const long long *__restrict__ off_m,
-    const long long *__restrict__ off_n, double alpha, double beta, int *__restrict__ status)
+    int M, int N, int mtiles, int ntiles, int kblocks, int kb_per_split, double *__restrict__ out,
+    const long long *__restrict__ off_m, const long long *__restrict__ off_n, double alpha, double beta,
+    double *__restrict__ partial, int *__restrict__ status)
 {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     __shared__ __align__(8) uint64_t full_bar[TC_STAGES], empty_bar[TC_STAGES], accf_bar[2], acce_bar[2];
     __shared__ uint32_t tmem_base_s;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.y * TC_BM, n0 = blockIdx.x * TC_BN;
+    // raster: groups of TC_GROUP_M row tiles, row tile fastest inside a group, so
+    // the CTAs resident at one time share a few A row tiles and each B tile is
+    // fetched from HBM about once
+    // (split-K: block = split * tiles + tile; split s covers k blocks
+    // [s * kb_per_split, min(kblocks, (s + 1) * kb_per_split)) and writes its
+    // FP64 partial tile to partial[s][M][N] for splitk_reduce_kernel)
+    const int tiles = mtiles * ntiles;
+    const int split = blockIdx.x / tiles;
+    const int tile = blockIdx.x - split * tiles;
+    const int group = tile / (TC_GROUP_M * ntiles);
+    const int first_m = group * TC_GROUP_M;
+    const int gsize = min(mtiles - first_m, TC_GROUP_M);
+    const int local = tile - group * TC_GROUP_M * ntiles;
+    const int m0 = (first_m + local % gsize) * TC_BM, n0 = (local / gsize) * TC_BN;
+    const int kb_begin = split * kb_per_split;
+    const int nkb = min(kblocks - kb_begin, kb_per_split);
     constexpr int KB_ELEMS = TC_ROWB / (KIND == KIND_TF32 ? 4 : 2);   // k per pipeline stage
     constexpr int KB_PER_CHUNK = TC_CHUNK_K / KB_ELEMS;
-    const int nchunks = (kblocks + KB_PER_CHUNK - 1) / KB_PER_CHUNK;
+    const int nchunks = (nkb + KB_PER_CHUNK - 1) / KB_PER_CHUNK;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < TC_STAGES; s++) {
@@ -189,7 +212,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_split_gemm_kernel(
         }
         for (int b = 0; b < 2; b++) {
             mbar_init(&accf_bar[b], 1);
-            mbar_init(&acce_bar[b], 4);
+            mbar_init(&acce_bar[b], TC_DRAIN_WARPS);
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -206,13 +229,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_split_gemm_kernel(
     if (warp == 0) {
         if (lane == 0) {
             // ---- TMA producer
-            for (int kb = 0; kb < kblocks; kb++) {
+            for (int kb = 0; kb < nkb; kb++) {
                 const int s = kb % TC_STAGES;
                 const uint32_t ph = (kb / TC_STAGES) & 1;
                 if (!mbar_wait(&empty_bar[s], ph ^ 1, status, 1)) break;
                 uint8_t *st = smem + s * TC_STAGE_BYTES;
                 mbar_expect_tx(&full_bar[s], TC_STAGE_BYTES);
-                const int kx = kb * KB_ELEMS;
+                const int kx = (kb_begin + kb) * KB_ELEMS;
                 tma_load_2d(&map_ahi, &full_bar[s], st, kx, m0);
                 tma_load_2d(&map_alo, &full_bar[s], st + TC_TILE_BYTES, kx, m0);
                 tma_load_2d(&map_bhi, &full_bar[s], st + 2 * TC_TILE_BYTES, kx, n0);
@@ -230,7 +253,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_split_gemm_kernel(
                 if (!mbar_wait(&acce_bar[buf], (use & 1) ^ 1, status, 2)) break;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const uint32_t acc_tmem = tmem + buf * TC_BN;
-                const int kb0 = c * KB_PER_CHUNK, kb1 = min(kblocks, kb0 + KB_PER_CHUNK);
+                const int kb0 = c * KB_PER_CHUNK, kb1 = min(nkb, kb0 + KB_PER_CHUNK);
                 for (int kb = kb0; kb < kb1; kb++) {
                     const int s = kb % TC_STAGES;
                     const uint32_t ph = (kb / TC_STAGES) & 1;
@@ -253,39 +276,50 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_split_gemm_kernel(
             }
         }
     } else {
-        // ---- drain warps
+        // ---- drain warps: FP64 running sums in registers, one write at the end
         const int q = warp & 3;
+        const int cbase = 64 * ((warp - 2) >> 2);
         const int m = m0 + q * 32 + lane;
-        const long long om = m < M ? off_m[m] : 0;
+        double sum[64];
+#pragma unroll
+        for (int i = 0; i < 64; i++) sum[i] = 0.0;
+        bool ok = true;
         for (int c = 0; c < nchunks; c++) {
             const int buf = c & 1;
             const uint32_t use = (uint32_t)(c >> 1);
             const bool got = mbar_wait(&accf_bar[buf], use & 1, status, 4);
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             // warp-uniform: tcgen05.ld is a .sync.aligned instruction
-            if (!__all_sync(0xffffffffu, got && *(volatile int *)status == 0)) break;
-#pragma unroll 1
-            for (int c0 = 0; c0 < TC_BN; c0 += 16) {
-                float v[16];
-                tmem_ld16(tmem + buf * TC_BN + ((uint32_t)(q * 32) << 16) + c0, v);
-                if (m < M) {
+            if (!__all_sync(0xffffffffu, got && *(volatile int *)status == 0)) { ok = false; break; }
 #pragma unroll
-                    for (int i = 0; i < 16; i++) {
-                        const int n = n0 + c0 + i;
-                        if (n < N) {
-                            double *o = out + om + off_n[n];
-                            const double val = alpha * (double)v[i];
-                            if (c == 0)
-                                *o = beta == 0.0 ? val : fma(beta, *o, val);
-                            else
-                                *o += val;
-                        }
-                    }
-                }
+            for (int c0 = 0; c0 < 64; c0 += 16) {
+                float v[16];
+                tmem_ld16(tmem + buf * TC_BN + ((uint32_t)(q * 32) << 16) + cbase + c0, v);
+#pragma unroll
+                for (int i = 0; i < 16; i++) sum[c0 + i] += (double)v[i];
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncwarp();
             if (lane == 0) mbar_arrive(&acce_bar[buf]);
+        }
+        if (ok && m < M && partial) {
+            double *p = partial + ((size_t)split * M + m) * N;
+#pragma unroll
+            for (int i = 0; i < 64; i++) {
+                const int n = n0 + cbase + i;
+                if (n < N) p[n] = sum[i];
+            }
+        } else if (ok && m < M) {
+            const long long om = off_m[m];
+#pragma unroll
+            for (int i = 0; i < 64; i++) {
+                const int n = n0 + cbase + i;
+                if (n < N) {
+                    double *o = out + om + off_n[n];
+                    const double val = alpha * sum[i];
+                    *o = beta == 0.0 ? val : fma(beta, *o, val);
+                }
+            }
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -293,6 +327,22 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_split_gemm_kernel(
     if (warp == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * TC_BN));
+    }
+}
+
+// ---- split-K reduction: out = alpha * sum_s partial[s] + beta * out (fixed order) ----
+__global__ void splitk_reduce_kernel(const double *__restrict__ partial, int ksplit, int M, int N,
+                                     double *__restrict__ out, const long long *__restrict__ off_m,
+                                     const long long *__restrict__ off_n, double alpha, double beta)
+{
+    const long long mn = (long long)M * N;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < mn;
+         e += (long long)gridDim.x * blockDim.x) {
+        double acc = 0.0;
+        for (int s = 0; s < ksplit; s++) acc += partial[s * mn + e];
+        const int m = (int)(e / N), n = (int)(e - (long long)m * N);
+        double *o = out + off_m[m] + off_n[n];
+        *o = beta == 0.0 ? alpha * acc : fma(beta, *o, alpha * acc);
     }
 }
 
@@ -372,16 +422,25 @@ static int make_map(CUtensorMap *map, const void *base, int kind, int rows_pad, 
 template <int KIND>
 static int launch_tc(const CUtensorMap &ma, const CUtensorMap &mal, const CUtensorMap &mb, const CUtensorMap &mbl,
                      int M, int N, int m_pad, int n_pad, int kblocks, double *out, const long long *off_m,
-                     const long long *off_n, double alpha, double beta, int *status, cudaStream_t st)
+                     const long long *off_n, double alpha, double beta, int ksplit, double *partial, int *status,
+                     cudaStream_t st)
 {
     const size_t smem = TC_STAGES * TC_STAGE_BYTES + 1024;
     if (cudaFuncSetAttribute(tc_split_gemm_kernel<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
         cudaSuccess)
         return check_launch("cudaFuncSetAttribute(tc_split_gemm_kernel)");
-    dim3 grid(n_pad / TC_BN, m_pad / TC_BM);
-    tc_split_gemm_kernel<KIND><<<grid, TC_THREADS, smem, st>>>(ma, mal, mb, mbl, M, N, kblocks, out, off_m, off_n,
-                                                                alpha, beta, status);
-    return check_launch("tc_split_gemm_kernel");
+    const int mt = m_pad / TC_BM, nt = n_pad / TC_BN;
+    const int per = (kblocks + ksplit - 1) / ksplit;
+    const int nsplit = (kblocks + per - 1) / per;           // every split non-empty
+    tc_split_gemm_kernel<KIND><<<(unsigned)((long long)mt * nt * nsplit), TC_THREADS, smem, st>>>(
+        ma, mal, mb, mbl, M, N, mt, nt, kblocks, per, out, off_m, off_n, alpha, beta, nsplit > 1 ? partial : nullptr,
+        status);
+    int rc = check_launch("tc_split_gemm_kernel");
+    if (rc || nsplit == 1) return rc;
+    const long long mn = (long long)M * N;
+    const int blocks = (int)std::min<long long>((mn + 255) / 256, 148ll * 16);
+    splitk_reduce_kernel<<<blocks, 256, 0, st>>>(partial, nsplit, M, N, out, off_m, off_n, alpha, beta);
+    return check_launch("splitk_reduce_kernel");
 }
 
 }  // namespace cb
@@ -416,12 +475,18 @@ int ccsd_b200_split_pack(int kind, const double *src1, const long long *o1r, con
 
 int ccsd_b200_tc_split_gemm(int kind, const void *a_hi, const void *a_lo, const void *b_hi, const void *b_lo, int M,
                             int N, int m_pad, int n_pad, int k_pad, double *out, const long long *off_m,
-                            const long long *off_n, double alpha, double beta, int *status, void *stream)
+                            const long long *off_n, double alpha, double beta, int ksplit, double *partial,
+                            int *status, void *stream)
 {
     const int kstep = TC_ROWB / (kind == KIND_TF32 ? 4 : 2);
+    if (ksplit < 1 || (ksplit > 1 && !partial) ||
+        (long long)(m_pad / TC_BM) * (n_pad / TC_BN) * ksplit > 2147483647ll) {
+        set_error("ccsd_b200_tc_split_gemm: invalid split-K arguments");
+        return CCSD_B200_ERR_ARG;
+    }
     if ((kind != KIND_TF32 && kind != KIND_BF16) || !a_hi || !a_lo || !b_hi || !b_lo || !out || !off_m || !off_n ||
         !status || M <= 0 || N <= 0 || m_pad < M || n_pad < N || m_pad % TC_BM || n_pad % TC_BN || k_pad <= 0 ||
-        k_pad % kstep || n_pad / TC_BN > 2147483647 || m_pad / TC_BM > 65535) {
+        k_pad % kstep || (long long)(m_pad / TC_BM) * (n_pad / TC_BN) > 2147483647ll) {
         set_error("ccsd_b200_tc_split_gemm: invalid argument");
         return CCSD_B200_ERR_ARG;
     }
@@ -433,9 +498,9 @@ int ccsd_b200_tc_split_gemm(int kind, const void *a_hi, const void *a_lo, const 
     cudaStream_t st = (cudaStream_t)stream;
     if (kind == KIND_TF32)
         return launch_tc<KIND_TF32>(ma, mal, mb, mbl, M, N, m_pad, n_pad, k_pad / kstep, out, off_m, off_n, alpha,
-                                    beta, status, st);
+                                    beta, ksplit, partial, status, st);
     return launch_tc<KIND_BF16>(ma, mal, mb, mbl, M, N, m_pad, n_pad, k_pad / kstep, out, off_m, off_n, alpha, beta,
-                                status, st);
+                                ksplit, partial, status, st);
 }
 
 }  // extern "C"

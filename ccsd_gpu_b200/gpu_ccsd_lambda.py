@@ -24,7 +24,7 @@ import numpy as np
 import torch
 
 from . import _native
-from .contract import check_status, contract
+from .contract import check_status, contract, mark_constant
 
 DEFAULT_MODE = "tf32x3"
 
@@ -54,6 +54,7 @@ class DeviceEris:
         self.ovvv = _t(ovvv, dev)
         self.vvvv = _t(eris.vvvv, dev) if getattr(eris, "vvvv", None) is not None else None
         self.nocc = self.ovoo.shape[0]
+        mark_constant(self.oooo, self.ovoo, self.ovvo, self.oovv, self.ovov, self.ovvv, self.vvvv)
 
     @classmethod
     def wrap(cls, eris):
@@ -149,6 +150,7 @@ def make_intermediates_gpu(mycc, t1, t2, eris, mode=None):
     E("laki,klbc->abic", g2ovoo, tau, out=wvvov, beta=1.0)
     E("ckjb,kc->bj", ov2, t1, out=w3, beta=1.0)
     w3 += w1 @ t1.T - t1.T @ w2
+    mark_constant(woooo, wvooo, wVOov, wvOOv, wvvov)
     return SimpleNamespace(w1=w1, w2=w2, w3=w3, w4=w4, woooo=woooo, wvooo=wvooo, wVOov=wVOov, wvOOv=wvOOv,
                            wvvov=wvvov, mode=E.mode)
 
@@ -282,6 +284,9 @@ def kernel_gpu(mycc, eris=None, t1=None, t2=None, l1=None, l2=None, max_cycle=No
     mode = _mode_of(mycc, mode)
     polish = getattr(mycc, "lambda_polish", True) if polish is None else polish
     t1g, t2g, l1g, l2g = _t(t1), _t(t2), _t(l1), _t(l2)
+    if t1g.data_ptr() == l1g.data_ptr() or t2g.data_ptr() == l2g.data_ptr():
+        l1g, l2g = l1g.clone(), l2g.clone()
+    mark_constant(t1g, t2g)
     cur_mode = mode
     cur_tol = tol if mode == "fp64" else max(tol, MIXED_FLOOR)
     imds = make_intermediates_gpu(mycc, t1g, t2g, eris, cur_mode)

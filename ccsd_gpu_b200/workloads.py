@@ -6,6 +6,7 @@ contraction coefficients uniform in [0.1, 1] then normalised with the PySCF
 convention, centres uniform in a 12-bohr cube, every shell on its own centre.
 """
 import numpy as np
+import torch
 
 from .gto.mole import BAS_SLOTS, PTR_ENV_START, normalized_coefficients
 
@@ -139,3 +140,70 @@ def quartet_flops(shells, q, deriv):
     for key, c in zip(keys, counts):
         total += int(c) * reference_flops(*[int(v) for v in key], deriv)
     return total
+
+
+# ---- synthetic CCSD state for the Lambda / 2-RDM contraction benchmark ----------------
+def _pair(a, b):
+    hi, lo = torch.maximum(a, b), torch.minimum(a, b)
+    return hi * (hi + 1) // 2 + lo
+
+
+def synthetic_eri_block(z, P, Q, R, S, decay=0.1, out=None):
+    """(pq|rs) over the index vectors P, Q, R, S of a symmetric random ERI tensor.
+
+    (pq|rs) = z[canonical(p, q, r, s)] * exp(-decay * D) with the orbital
+    distance D = |p-q| + |r-s| + (|p-r| + |q-s| + |p-s| + |q-r|) / 2: one random
+    value per unique index quartet and a D that is invariant under the 8
+    index permutations, so the tensor has the full 8-fold symmetry of real
+    orbitals.  Evaluated slice by slice in P.
+    """
+    dev = z.device
+    P, Q, R, S = (torch.as_tensor(x, dtype=torch.int64, device=dev) for x in (P, Q, R, S))
+    pq = _pair(P[:, None], Q[None, :])
+    rs = _pair(R[:, None], S[None, :])
+    dpq = (P[:, None] - Q[None, :]).abs()
+    drs = (R[:, None] - S[None, :]).abs()
+    if out is None:
+        out = torch.empty((len(P), len(Q), len(R), len(S)), dtype=torch.float64, device=dev)
+    for p in range(len(P)):
+        idx = _pair(pq[p][:, None, None], rs[None])
+        a = (P[p] - R).abs()[None, :, None] + (Q[:, None, None] - S[None, None, :]).abs()
+        b = (P[p] - S).abs()[None, None, :] + (Q[:, None, None] - R[None, :, None]).abs()
+        dist = dpq[p][:, None, None] + drs[None] + 0.5 * (a + b)
+        out[p] = z[idx] * torch.exp(-decay * dist.double())
+    return out
+
+
+def lambda_bench_state(nocc=24, nvir=216, seed=0, device="cuda", eri_sigma=0.05, decay=0.1):
+    """Seeded synthetic CCSD state with PySCF's RCCSD integral layout.
+
+    Orbital energies: sorted uniform in [-2, -0.3] Eh (occupied) and [0.1, 5] Eh
+    (virtual); Fock matrix = diag(mo_energy).  t1 ~ N(0, 1e-3) and t2 ~ N(0,
+    1e-2) (symmetrised to t2[ijab] = t2[jiba]), scaled by 1/(1 + |e_a - e_i|) and
+    1/(1 + |e_a + e_b - e_i - e_j|).  MO ERIs: :func:`synthetic_eri_block` with
+    values N(0, eri_sigma), decay constant 0.1 per orbital index step.  Returns
+    (eris, t1, t2) with eris.{fock, mo_energy, oooo, ovoo, ovvo, oovv, ovov,
+    ovvv, vvvv} as float64 tensors on ``device``.
+    """
+    from types import SimpleNamespace
+    dev = torch.device(device)
+    g = torch.Generator(device=dev).manual_seed(seed)
+    nmo = nocc + nvir
+    eo = torch.sort(torch.rand(nocc, generator=g, device=dev, dtype=torch.float64) * 1.7 - 2.0).values
+    ev = torch.sort(torch.rand(nvir, generator=g, device=dev, dtype=torch.float64) * 4.9 + 0.1).values
+    e = torch.cat([eo, ev])
+    npair = nmo * (nmo + 1) // 2
+    z = torch.randn(npair * (npair + 1) // 2, generator=g, device=dev, dtype=torch.float64) * eri_sigma
+    o = torch.arange(nocc, device=dev)
+    v = torch.arange(nocc, nmo, device=dev)
+    blk = lambda a, b, c, d: synthetic_eri_block(z, a, b, c, d, decay)   # noqa: E731
+    eris = SimpleNamespace(fock=torch.diag(e), mo_energy=e, oooo=blk(o, o, o, o), ovoo=blk(o, v, o, o),
+                           ovvo=blk(o, v, v, o), oovv=blk(o, o, v, v), ovov=blk(o, v, o, v),
+                           ovvv=blk(o, v, v, v), vvvv=blk(v, v, v, v))
+    del z
+    eia = eo[:, None] - ev[None, :]
+    t1 = torch.randn(nocc, nvir, generator=g, device=dev, dtype=torch.float64) * 1e-3 / (1 + eia.abs())
+    x = torch.randn(nocc, nocc, nvir, nvir, generator=g, device=dev, dtype=torch.float64)
+    d2 = (eia[:, None, :, None] + eia[None, :, None, :]).abs()
+    t2 = (x + x.permute(1, 0, 3, 2)) * (1e-2 / np.sqrt(2.0)) / (1 + d2)
+    return eris, t1, t2

@@ -142,14 +142,20 @@ int ccsd_b200_split_pack(int kind, const double *src1, const long long *o1r, con
  * for m < M, n < N.  The tensor cores accumulate in FP32 over chunks of
  * 512 k; each chunk is added to the output in FP64.  Operands come from
  * ccsd_b200_split_pack (A: [m_pad x k_pad], B: [n_pad x k_pad], m_pad and
- * n_pad multiples of 128).  `status` (one int, zero-initialised by the
+ * n_pad multiples of 128).  Split-K: with ksplit > 1 the k blocks are
+ * divided over up to ksplit CTAs per output tile; each writes an FP64
+ * partial tile into `partial` (caller-allocated, ksplit * M * N doubles) and a
+ * second kernel sums the partials in a fixed order and applies alpha/beta, so
+ * results do not depend on scheduling.  ksplit = 1 needs no `partial`.
+ * `status` (one int, zero-initialised by the
  * caller) receives a non-zero code if a pipeline wait expired.  Replaces the
  * cuTENSOR/cuBLAS einsum contractions of the Lambda solver and density
  * builders, and the CPU vvvv ladder term (ref: ccsd_gpu/gpu_ccsd_lambda.py:238-241).
  */
 int ccsd_b200_tc_split_gemm(int kind, const void *a_hi, const void *a_lo, const void *b_hi, const void *b_lo,
                             int M, int N, int m_pad, int n_pad, int k_pad, double *out, const long long *off_m,
-                            const long long *off_n, double alpha, double beta, int *status, void *stream);
+                            const long long *off_n, double alpha, double beta, int ksplit, double *partial,
+                            int *status, void *stream);
 
 #ifdef __cplusplus
 }

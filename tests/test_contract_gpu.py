@@ -56,3 +56,54 @@ def test_fp64_mode_is_einsum():
     a = torch.randn(7, 8, dtype=torch.float64, device="cuda")
     b = torch.randn(9, 8, dtype=torch.float64, device="cuda")
     assert torch.allclose(contract("mk,nk->mn", a, b, mode="fp64"), a @ b.T, rtol=1e-14, atol=1e-14)
+
+
+def test_tall_skinny_more_than_65535_row_tiles():
+    """M = 8.4M rows (65,600 row tiles of 128): the 1-D tile raster covers it
+    (the gvvvv . t1 contraction of the 2-RDM at nvir = 216 has 78,732)."""
+    from ccsd_gpu_b200.contract import check_status, contract
+    g = torch.Generator(device="cuda").manual_seed(3)
+    M, N, K = 128 * 65600, 24, 16
+    a = torch.randn(M, K, dtype=torch.float64, device="cuda", generator=g)
+    b = torch.randn(N, K, dtype=torch.float64, device="cuda", generator=g)
+    got = contract("mk,nk->mn", a, b)
+    check_status()
+    assert _rel(got, a @ b.T) < 5e-6
+
+
+def test_packed_operand_cache_follows_in_place_updates():
+    from ccsd_gpu_b200.contract import _pack_cache, check_status, contract, mark_constant
+    g = torch.Generator(device="cuda").manual_seed(4)
+    a = torch.randn(300, 200, dtype=torch.float64, device="cuda", generator=g)
+    b = torch.randn(100, 200, dtype=torch.float64, device="cuda", generator=g)
+    mark_constant(b)
+    n0 = len(_pack_cache)
+    r1 = contract("mk,nk->mn", a, b)
+    assert len(_pack_cache) == n0 + 1
+    r2 = contract("mk,nk->mn", a, b)
+    assert torch.equal(r1, r2)
+    b.mul_(2.0)                       # bumps the version counter: the packed copy is stale
+    r3 = contract("mk,nk->mn", a, b)
+    check_status()
+    assert _rel(r3, a @ b.T) < 5e-6
+    del b
+    assert len(_pack_cache) <= n0 + 1
+
+
+def test_split_k_skinny_output_long_k():
+    """Output of 2 x 1 tiles with K = 300,000: the k blocks are split over
+    CTAs (partials summed in a fixed order by a second kernel); beta applied once."""
+    from ccsd_gpu_b200.contract import STATS, check_status, contract
+    g = torch.Generator(device="cuda").manual_seed(5)
+    M, N, K = 200, 24, 300000
+    a = torch.randn(M, K, dtype=torch.float64, device="cuda", generator=g)
+    b = torch.randn(N, K, dtype=torch.float64, device="cuda", generator=g)
+    out = torch.randn(M, N, dtype=torch.float64, device="cuda", generator=g)
+    ref = 0.25 * out + 2.0 * (a @ b.T)
+    n0 = STATS["launches"]
+    contract("mk,nk->mn", a, b, out=out, alpha=2.0, beta=0.25)
+    check_status()
+    assert STATS["launches"] - n0 == 4          # two packs, GEMM, split-K reduction
+    assert _rel(out, ref) < 5e-6
+    again = contract("mk,nk->mn", a, b)
+    assert torch.equal(again, contract("mk,nk->mn", a, b))   # fixed summation order
