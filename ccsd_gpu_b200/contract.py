@@ -29,7 +29,8 @@ from . import _native
 KIND = {"tf32x3": 0, "bf16x3": 1}
 MODES = ("fp64", "tf32x3", "bf16x3")
 _BM = 128
-_KALIGN = {"tf32x3": 32, "bf16x3": 64}
+_KALIGN = {"tf32x3": 4, "bf16x3": 8}      # packed rows start on 16-byte boundaries
+_KSTEP = {"tf32x3": 32, "bf16x3": 64}     # k per 128-byte TMA box row
 
 
 def _parse(spec):
@@ -186,6 +187,38 @@ def _pack_new(terms, sub, rows_idx, k_idx, shape_map, kind, rows_pad, k_pad, dev
     return hi, lo
 
 
+# split-precision modes send a contraction to FP64 cuBLAS when its reduction
+# is this short, or when its arithmetic intensity (FP64 flop per operand/result
+# byte) is below LOW_INTENSITY_FLOP_PER_BYTE and K is at most
+# LOW_INTENSITY_MAX_K: such shapes are bound by HBM, not by the tensor cores.
+# Long, skinny reductions stay on the split-K tensor-core route (cuBLAS
+# parallelises them poorly, and their large operands stay packed in the cache).
+LOW_INTENSITY_K = 32
+LOW_INTENSITY_FLOP_PER_BYTE = 12.0
+LOW_INTENSITY_MAX_K = 1024
+
+
+def _combine(terms):
+    (c, t), rest = terms[0], terms[1:]
+    x = t * c if c != 1.0 or rest else t
+    for c2, t2 in rest:
+        x = x.add_(t2, alpha=c2)
+    return x
+
+
+def _fp64_contract(spec, ta, tb, shape_map, out, alpha, beta):
+    """out = alpha * einsum(spec, a, b) + beta * out with torch.einsum (cuBLAS
+    DGEMM); two-term operands are formed first, as the FP64 reference path does."""
+    STATS["flops"] += 2 * int(np.prod(list(shape_map.values())))
+    STATS["gemms"] += 1
+    res = torch.einsum(spec, _combine(ta), _combine(tb))
+    if beta == 0.0:
+        out.copy_(res * alpha if alpha != 1.0 else res)
+    else:
+        out.mul_(beta).add_(res, alpha=alpha)
+    return out
+
+
 def contract(spec, a, b, out=None, alpha=1.0, beta=0.0, mode="tf32x3", stream=None):
     """out[...] = alpha * einsum(spec, a, b) + beta * out  (returns out)."""
     ta, tb = _terms(a), _terms(b)
@@ -205,19 +238,7 @@ def contract(spec, a, b, out=None, alpha=1.0, beta=0.0, mode="tf32x3", stream=No
         out = torch.zeros([shape_map[i] for i in so], dtype=torch.float64, device=dev)
         beta = 0.0
     if mode == "fp64":
-        n_all = int(np.prod(list(shape_map.values())))
-        STATS["flops"] += 2 * n_all * len(ta) * len(tb)
-        STATS["gemms"] += len(ta) * len(tb)
-        res = None
-        for c1, t1 in ta:
-            for c2, t2 in tb:
-                r = torch.einsum(spec, t1, t2) * (c1 * c2)
-                res = r if res is None else res + r
-        if beta == 0.0:
-            out.copy_(res * alpha)
-        else:
-            out.mul_(beta).add_(res, alpha=alpha)
-        return out
+        return _fp64_contract(spec, ta, tb, shape_map, out, alpha, beta)
     if mode not in KIND:
         raise ValueError("unknown mode %r" % mode)
     _native.require_cuda(out)
@@ -243,10 +264,14 @@ def contract(spec, a, b, out=None, alpha=1.0, beta=0.0, mode="tf32x3", stream=No
     K = int(np.prod([shape_map[i] for i in k_idx])) if k_idx else 1
     if M == 0 or N == 0:
         return out
+    if K <= LOW_INTENSITY_K or (K <= LOW_INTENSITY_MAX_K and 2.0 * M * N * K <
+                                LOW_INTENSITY_FLOP_PER_BYTE * 8.0 * (M * K + N * K + M * N)):
+        # memory-bound shape: FP64 through cuBLAS moves fewer bytes than the
+        # split/pack/tensor-core route and is exact to FP64
+        return _fp64_contract(spec, ta, tb, shape_map, out, alpha, beta)
     kind = KIND[mode]
     kal = _KALIGN[mode]
-    m_pad = -(-M // _BM) * _BM
-    n_pad = -(-N // _BM) * _BM
+    m_pad, n_pad = M, N                    # tiles past M / N are zero-filled by TMA
     k_pad = max(kal, -(-K // kal) * kal)
     st = _native.stream(stream)
     ahi, alo = _pack(ta, sa, m_idx, k_idx, shape_map, kind, m_pad, k_pad, dev, st)
@@ -255,7 +280,7 @@ def contract(spec, a, b, out=None, alpha=1.0, beta=0.0, mode="tf32x3", stream=No
     key_n = ("on", tuple(n_idx), so, tuple(out.stride()), tuple(shape_map[i] for i in n_idx))
     om = _dev_offsets(key_m, lambda: _offsets(m_idx, so, shape_map, out), dev)
     on = _dev_offsets(key_n, lambda: _offsets(n_idx, so, shape_map, out), dev)
-    ksplit = _ksplit(m_pad, n_pad, k_pad // kal, dev)
+    ksplit = _ksplit(m_pad, n_pad, -(-k_pad // _KSTEP[mode]), dev)
     partial = torch.empty(ksplit * M * N, dtype=torch.float64, device=dev) if ksplit > 1 else None
     STATS["flops"] += 2 * M * N * K
     STATS["gemms"] += 1
@@ -276,7 +301,7 @@ def _ksplit(m_pad, n_pad, kblocks, dev):
     sms = _sm_count.get(dev)
     if sms is None:
         sms = _sm_count[dev] = torch.cuda.get_device_properties(dev).multi_processor_count
-    tiles = (m_pad // _BM) * (n_pad // _BM)
+    tiles = -(-m_pad // _BM) * -(-n_pad // _BM)
     if tiles >= sms or kblocks < 2 * _KB_PER_CHUNK:
         return 1
     return int(max(1, min(-(-2 * sms // tiles), kblocks // _KB_PER_CHUNK)))

@@ -14,7 +14,11 @@
 // Operands are produced by split_pack_kernel: it gathers an FP64 operand (up
 // to two linear terms, each addressed through offset tables, so transposes and
 // "2 t - t^T" combinations fuse into the pack), splits every value into hi and
-// lo parts and writes K-major, zero-padded [rows_pad x k_pad] arrays for TMA.
+// lo parts and writes K-major [rows_pad x k_pad] arrays for TMA (k_pad: K
+// rounded up to a 16-byte row; the values past K are zero).  Rows past the
+// array and k past k_pad are not stored: TMA fills the out-of-bounds part of
+// a 128 x 128-byte box with zeros, so skinny operands (24 rows, or K = 24)
+// cost only their own bytes.
 //
 // CTA = 320 threads, one 128 x 128 output tile:
 //   warp 0      TMA producer (lane 0) into a 3-stage ring of {A_hi, A_lo, B_hi,
@@ -47,6 +51,8 @@ static constexpr int TC_DRAIN_WARPS = 8;                // 2 per TMEM lane quadr
 static constexpr int TC_THREADS = 64 + 32 * TC_DRAIN_WARPS;
 static constexpr int TC_CHUNK_K = 512;                   // k per FP32 accumulation chunk
 static constexpr int TC_GROUP_M = 8;                     // row tiles per raster group
+static constexpr int TC_EPI_LD = 65;                     // epilogue staging row stride (doubles)
+static_assert(TC_DRAIN_WARPS * 32 * TC_EPI_LD * 8 <= TC_STAGES * TC_STAGE_BYTES, "epilogue staging fits the ring");
 static constexpr unsigned long long TC_WAIT_NS = 2000000000ull;
 
 enum { KIND_TF32 = 0, KIND_BF16 = 1 };
@@ -277,9 +283,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_split_gemm_kernel(
         }
     } else {
         // ---- drain warps: FP64 running sums in registers, one write at the end
+        //      (lane = output row of the TMEM lane quadrant q)
         const int q = warp & 3;
         const int cbase = 64 * ((warp - 2) >> 2);
-        const int m = m0 + q * 32 + lane;
         double sum[64];
 #pragma unroll
         for (int i = 0; i < 64; i++) sum[i] = 0.0;
@@ -302,22 +308,32 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_split_gemm_kernel(
             __syncwarp();
             if (lane == 0) mbar_arrive(&acce_bar[buf]);
         }
-        if (ok && m < M && partial) {
-            double *p = partial + ((size_t)split * M + m) * N;
+        // Epilogue through shared memory: once the last chunk has been read,
+        // every MMA of this tile has completed, so the stage ring is free.  Each
+        // warp stores its 32 x 64 block row-major (stride 65: conflict-free in
+        // both directions) and writes it back one output row at a time, lanes
+        // along n: coalesced whenever off_n is contiguous.
+        if (ok) {
+            double *blk = reinterpret_cast<double *>(smem) + (warp - 2) * (32 * TC_EPI_LD);
 #pragma unroll
-            for (int i = 0; i < 64; i++) {
-                const int n = n0 + cbase + i;
-                if (n < N) p[n] = sum[i];
-            }
-        } else if (ok && m < M) {
-            const long long om = off_m[m];
+            for (int i = 0; i < 64; i++) blk[lane * TC_EPI_LD + i] = sum[i];
+            __syncwarp();
+            const int mrow0 = m0 + q * 32;
+            for (int r = 0; r < 32 && mrow0 + r < M; r++) {
+                const int mr = mrow0 + r;
+                const long long om = partial ? 0 : off_m[mr];
 #pragma unroll
-            for (int i = 0; i < 64; i++) {
-                const int n = n0 + cbase + i;
-                if (n < N) {
-                    double *o = out + om + off_n[n];
-                    const double val = alpha * sum[i];
-                    *o = beta == 0.0 ? val : fma(beta, *o, val);
+                for (int h = 0; h < 2; h++) {
+                    const int c = lane + 32 * h;
+                    const int n = n0 + cbase + c;
+                    if (n >= N) continue;
+                    const double v = blk[r * TC_EPI_LD + c];
+                    if (partial) {
+                        partial[((size_t)split * M + mr) * N + n] = v;
+                    } else {
+                        double *o = out + om + off_n[n];
+                        *o = beta == 0.0 ? alpha * v : fma(beta, *o, alpha * v);
+                    }
                 }
             }
         }
@@ -429,7 +445,7 @@ static int launch_tc(const CUtensorMap &ma, const CUtensorMap &mal, const CUtens
     if (cudaFuncSetAttribute(tc_split_gemm_kernel<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
         cudaSuccess)
         return check_launch("cudaFuncSetAttribute(tc_split_gemm_kernel)");
-    const int mt = m_pad / TC_BM, nt = n_pad / TC_BN;
+    const int mt = (m_pad + TC_BM - 1) / TC_BM, nt = (n_pad + TC_BN - 1) / TC_BN;
     const int per = (kblocks + ksplit - 1) / ksplit;
     const int nsplit = (kblocks + per - 1) / per;           // every split non-empty
     tc_split_gemm_kernel<KIND><<<(unsigned)((long long)mt * nt * nsplit), TC_THREADS, smem, st>>>(
@@ -454,8 +470,8 @@ int ccsd_b200_split_pack(int kind, const double *src1, const long long *o1r, con
                          int rows_pad, int k_pad, void *hi, void *lo, void *stream)
 {
     if ((kind != KIND_TF32 && kind != KIND_BF16) || !src1 || !o1r || !o1k || rows < 0 || K < 0 ||
-        rows_pad < rows || k_pad < K || !hi || !lo || (src2 && (!o2r || !o2k)) || rows_pad % TC_BM ||
-        k_pad % (TC_ROWB / (kind == KIND_TF32 ? 4 : 2))) {
+        rows_pad < rows || k_pad < K || !hi || !lo || (src2 && (!o2r || !o2k)) ||
+        k_pad % (16 / (kind == KIND_TF32 ? 4 : 2))) {
         set_error("ccsd_b200_split_pack: invalid argument");
         return CCSD_B200_ERR_ARG;
     }
@@ -480,13 +496,13 @@ int ccsd_b200_tc_split_gemm(int kind, const void *a_hi, const void *a_lo, const 
 {
     const int kstep = TC_ROWB / (kind == KIND_TF32 ? 4 : 2);
     if (ksplit < 1 || (ksplit > 1 && !partial) ||
-        (long long)(m_pad / TC_BM) * (n_pad / TC_BN) * ksplit > 2147483647ll) {
+        (long long)((m_pad + TC_BM - 1) / TC_BM) * ((n_pad + TC_BN - 1) / TC_BN) * ksplit > 2147483647ll) {
         set_error("ccsd_b200_tc_split_gemm: invalid split-K arguments");
         return CCSD_B200_ERR_ARG;
     }
     if ((kind != KIND_TF32 && kind != KIND_BF16) || !a_hi || !a_lo || !b_hi || !b_lo || !out || !off_m || !off_n ||
-        !status || M <= 0 || N <= 0 || m_pad < M || n_pad < N || m_pad % TC_BM || n_pad % TC_BN || k_pad <= 0 ||
-        k_pad % kstep || (long long)(m_pad / TC_BM) * (n_pad / TC_BN) > 2147483647ll) {
+        !status || M <= 0 || N <= 0 || m_pad < M || n_pad < N || k_pad <= 0 ||
+        k_pad % (16 / (kind == KIND_TF32 ? 4 : 2))) {
         set_error("ccsd_b200_tc_split_gemm: invalid argument");
         return CCSD_B200_ERR_ARG;
     }
@@ -496,10 +512,11 @@ int ccsd_b200_tc_split_gemm(int kind, const void *a_hi, const void *a_lo, const 
         (rc = make_map(&mb, b_hi, kind, n_pad, k_pad)) || (rc = make_map(&mbl, b_lo, kind, n_pad, k_pad)))
         return rc;
     cudaStream_t st = (cudaStream_t)stream;
+    const int kblocks = (k_pad + kstep - 1) / kstep;
     if (kind == KIND_TF32)
-        return launch_tc<KIND_TF32>(ma, mal, mb, mbl, M, N, m_pad, n_pad, k_pad / kstep, out, off_m, off_n, alpha,
-                                    beta, ksplit, partial, status, st);
-    return launch_tc<KIND_BF16>(ma, mal, mb, mbl, M, N, m_pad, n_pad, k_pad / kstep, out, off_m, off_n, alpha, beta,
+        return launch_tc<KIND_TF32>(ma, mal, mb, mbl, M, N, m_pad, n_pad, kblocks, out, off_m, off_n, alpha, beta,
+                                    ksplit, partial, status, st);
+    return launch_tc<KIND_BF16>(ma, mal, mb, mbl, M, N, m_pad, n_pad, kblocks, out, off_m, off_n, alpha, beta,
                                 ksplit, partial, status, st);
 }
 

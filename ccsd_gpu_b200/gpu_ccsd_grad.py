@@ -110,8 +110,12 @@ def _gamma2_intermediates_gpu(mycc, t1, t2, l1, l2):
     dovov = 2 * goovv.permute(0, 2, 1, 3) - goovv.permute(1, 2, 0, 3)
     gvvvv = E("ijab,ijcd->abcd", l2, tau)          # l2 . (t2 + t1 t1)
     dvvvv = gvvvv.permute(0, 2, 1, 3) - 0.5 * gvvvv.permute(0, 3, 1, 2)
-    gvovv = E("adbc,id->aibc", gvvvv, t1, alpha=-1.0)
     del gvvvv
+    # gvovv[a,i,b,c] = -sum_d gvvvv[a,d,b,c] t1[i,d], evaluated as
+    # -sum_kl (sum_d l2[k,l,a,d] t1[i,d]) tau[k,l,b,c]: one tensor-core GEMM
+    # instead of a skinny product that re-reads a permuted nvir^4 array
+    xl2t1 = E("klad,id->klai", l2, t1)
+    gvovv = E("klai,klbc->aibc", xl2t1, tau, alpha=-1.0)
     E("akic,kb->aibc", pvoOV, t1, out=gvovv, beta=1.0)
     E("akib,kc->aibc", pvOOv, t1, out=gvovv, alpha=-1.0, beta=1.0)
     E("ja,jibc->aibc", l1, tau, out=gvovv, beta=1.0)

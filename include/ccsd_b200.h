@@ -126,7 +126,9 @@ int ccsd_b200_fp64_fma_probe(double *out, int blocks, int iters, void *stream);
  *   v[r][k] = c1 * src1[o1r[r] + o1k[k]] + c2 * src2[o2r[r] + o2k[k]]   (src2 may be NULL)
  * for r < rows, k < K (zero elsewhere), written as hi + lo parts, K-major,
  * [rows_pad x k_pad]: kind 0 = TF32 (float storage, 4 B), kind 1 = BF16 (2 B).
- * rows_pad must be a multiple of 128 and k_pad of 32 (TF32) / 64 (BF16).
+ * rows_pad >= rows; k_pad >= K and a multiple of 4 (TF32) / 8 (BF16), so
+ * that every row starts on a 16-byte boundary.  No padding to the 128-row
+ * GEMM tile is needed: the GEMM's TMA loads read zeros past the array.
  * The offset tables (int64, element units) express any strided or permuted
  * view of the FP64 operands.  Replaces the operand transposes/copies that
  * precede the CuPy einsum contractions of the Lambda and RDM builders
@@ -141,8 +143,8 @@ int ccsd_b200_split_pack(int kind, const double *src1, const long long *o1r, con
  *   out[off_m[m] + off_n[n]] = alpha * sum_k (Ahi Bhi + Ahi Blo + Alo Bhi)[m,n,k] + beta * out[...]
  * for m < M, n < N.  The tensor cores accumulate in FP32 over chunks of
  * 512 k; each chunk is added to the output in FP64.  Operands come from
- * ccsd_b200_split_pack (A: [m_pad x k_pad], B: [n_pad x k_pad], m_pad and
- * n_pad multiples of 128).  Split-K: with ksplit > 1 the k blocks are
+ * ccsd_b200_split_pack (A: [m_pad x k_pad], B: [n_pad x k_pad], m_pad >= M,
+ * n_pad >= N, k_pad a multiple of 4 (TF32) / 8 (BF16)).  Split-K: with ksplit > 1 the k blocks are
  * divided over up to ksplit CTAs per output tile; each writes an FP64
  * partial tile into `partial` (caller-allocated, ksplit * M * N doubles) and a
  * second kernel sums the partials in a fixed order and applies alpha/beta, so

@@ -18,7 +18,7 @@ def _rel(a, b):
 def test_plain_gemm(mode, tol):
     from ccsd_gpu_b200.contract import check_status, contract
     g = torch.Generator(device="cuda").manual_seed(0)
-    for M, N, K in [(128, 128, 32), (200, 300, 100), (1, 7, 5), (333, 129, 1000), (260, 140, 5000)]:
+    for M, N, K in [(128, 128, 40), (200, 300, 100), (333, 129, 1000), (260, 140, 5000), (1, 7, 5)]:
         a = torch.randn(M, K, dtype=torch.float64, device="cuda", generator=g)
         b = torch.randn(N, K, dtype=torch.float64, device="cuda", generator=g)
         ref = a @ b.T
@@ -95,7 +95,7 @@ def test_split_k_skinny_output_long_k():
     CTAs (partials summed in a fixed order by a second kernel); beta applied once."""
     from ccsd_gpu_b200.contract import STATS, check_status, contract
     g = torch.Generator(device="cuda").manual_seed(5)
-    M, N, K = 200, 24, 300000
+    M, N, K = 256, 64, 300000
     a = torch.randn(M, K, dtype=torch.float64, device="cuda", generator=g)
     b = torch.randn(N, K, dtype=torch.float64, device="cuda", generator=g)
     out = torch.randn(M, N, dtype=torch.float64, device="cuda", generator=g)
@@ -107,3 +107,33 @@ def test_split_k_skinny_output_long_k():
     assert _rel(out, ref) < 5e-6
     again = contract("mk,nk->mn", a, b)
     assert torch.equal(again, contract("mk,nk->mn", a, b))   # fixed summation order
+
+
+def test_memory_bound_shapes_take_the_fp64_route():
+    """K <= 32 or fewer than 12 flop per byte: FP64 cuBLAS, no native launch."""
+    from ccsd_gpu_b200.contract import STATS, contract
+    g = torch.Generator(device="cuda").manual_seed(6)
+    w = torch.randn(24, 24, dtype=torch.float64, device="cuda", generator=g)
+    l2 = torch.randn(24, 24, 30, 30, dtype=torch.float64, device="cuda", generator=g)
+    n0 = STATS["launches"]
+    got = contract("jk,kiba->jiba", w, l2)
+    assert STATS["launches"] == n0
+    assert torch.allclose(got, torch.einsum("jk,kiba->jiba", w, l2), rtol=1e-13, atol=1e-13)
+
+
+@pytest.mark.parametrize("mode,tol", [("tf32x3", 5e-6), ("bf16x3", 1e-4)])
+def test_tensor_route_on_tiny_and_ragged_shapes(mode, tol, monkeypatch):
+    """The tcgen05 route itself on shapes the dispatcher would send to FP64:
+    one row, K below one TMA box, rows past the operand read as zeros."""
+    import ccsd_gpu_b200.contract as C
+    monkeypatch.setattr(C, "LOW_INTENSITY_K", 0)
+    monkeypatch.setattr(C, "LOW_INTENSITY_FLOP_PER_BYTE", 0.0)
+    g = torch.Generator(device="cuda").manual_seed(7)
+    for M, N, K in [(1, 7, 5), (128, 128, 40), (24, 5000, 24), (3, 1, 1)]:
+        a = torch.randn(M, K, dtype=torch.float64, device="cuda", generator=g)
+        b = torch.randn(N, K, dtype=torch.float64, device="cuda", generator=g)
+        n0 = C.STATS["launches"]
+        got = C.contract("mk,nk->mn", a, b, mode=mode)
+        C.check_status()
+        assert C.STATS["launches"] - n0 >= 3
+        assert _rel(got, a @ b.T) < tol, (M, N, K)
