@@ -16,8 +16,12 @@ Other workloads (``--workload``):
           2-RDM blocks against the FP64 run.
   gemm    the split-precision tcgen05 GEMM alone (4096^3 and the vvvv-ladder
           shape 576 x 46656 x 46656) against cuBLAS DGEMM.
+  grad    RHF-CCSD analytic nuclear gradient of H2O/cc-pVDZ (O at the origin,
+          H at (0, +-0.757, 0.587) A): RHF + CCSD + Lambda + gradient per step,
+          FP64 mode and the split-precision mode; grads/s and max|dg| between
+          them; the numpy restatement of the same chain timed on the host.
 
-  python bench.py [--workload eri|lambda|gemm] [--gpus N] [--steps K] [--warmup W]
+  python bench.py [--workload eri|lambda|gemm|grad] [--gpus N] [--steps K] [--warmup W]
                   [--impl ours|reference]
 
 Multi-GPU (torchrun): every rank runs its own copy of the workload (weak
@@ -42,7 +46,7 @@ NSHELL = 4096
 
 def parse():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", choices=["eri", "lambda", "gemm"], default="eri")
+    ap.add_argument("--workload", choices=["eri", "lambda", "gemm", "grad"], default="eri")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=None)
@@ -56,7 +60,7 @@ def parse():
     ap.add_argument("--quartets", type=int, default=1 << 18, help="sampled quartets per rank per step")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU-baseline sample budget")
     args = ap.parse_args()
-    dflt = {"eri": (10, 3), "lambda": (3, 3), "gemm": (10, 3)}[args.workload]
+    dflt = {"eri": (10, 3), "lambda": (3, 3), "gemm": (10, 3), "grad": (5, 3)}[args.workload]
     args.steps = dflt[0] if args.steps is None else args.steps
     args.warmup = dflt[1] if args.warmup is None else args.warmup
     return args
@@ -357,6 +361,70 @@ def run_lambda(args, ws, rank, local):
         print(json.dumps(line), flush=True)
 
 
+
+H2O_CCPVDZ = "O 0 0 0; H 0 0.757 0.587; H 0 -0.757 0.587"
+
+
+def run_grad(args, ws, rank, local):
+    """Full CCSD gradient of H2O/cc-pVDZ per step, FP64 vs split precision."""
+    from ccsd_gpu_b200.ccsd import CCSD
+    from ccsd_gpu_b200.contract import STATS, reset_stats
+    from ccsd_gpu_b200.gto import M
+    from ccsd_gpu_b200.scf import RHF
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    barrier = (lambda: (torch.distributed.barrier(), torch.cuda.synchronize(dev))) if ws > 1 else \
+        (lambda: torch.cuda.synchronize(dev))
+    mol = M(atom=H2O_CCPVDZ, basis="cc-pvdz")
+    grads = {}
+
+    def step(mode):
+        def run():
+            cc = CCSD(RHF(mol).run(), precision=mode)
+            cc.kernel()
+            cc.conv_tol_normt = 1e-9
+            grads[mode] = cc.nuc_grad_method().kernel()        # numpy (natm, 3): the D2H read
+        return run
+
+    res = {}
+    for mode in ("fp64", args.mode):
+        fn = step(mode)
+        for _ in range(args.warmup):
+            fn()
+        reset_stats()
+        with ClockSampler(dev) as clk:
+            ks, _ = _events_timed(fn, args.steps, barrier)
+        res[mode] = {"s_per_grad": _maxr(float(ks.mean()), ws, dev) * 1e-3, "clocks": clk.summary(),
+                     "launches": STATS["launches"] // args.steps}
+    dg = float(np.abs(grads[args.mode] - grads["fp64"]).max())
+    cpu = None
+    if rank == 0 and ws == 1:
+        from oracle import scf_cc_oracle as Q
+        t = time.perf_counter()
+        _, g_ref = Q.ccsd_gradient(mol)
+        dt = time.perf_counter() - t
+        cpu = {"value": 1.0 / dt, "unit": "grads/s", "cores": int(torch.get_num_threads()), "kind": "port",
+               "sample": "one H2O/cc-pVDZ CCSD gradient by the numpy restatement of the chain (%.1f s)" % dt,
+               "max_abs_dg_fp64_gpu_vs_port": float(np.abs(grads["fp64"] - g_ref).max())}
+    mx = res[args.mode]
+    line = {"metric": "CCSD grads/s, H2O/cc-pVDZ (RHF + CCSD + Lambda + gradient per step), %s vs FP64" % args.mode,
+            "value": ws / mx["s_per_grad"], "unit": "grads/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": mx["s_per_grad"] * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": args.mode, "data": "synthetic",
+            "config": {"workload": "h2o_ccpvdz_ccsd_gradient", "nao": mol.nao_nr(), "nocc": mol.nelectron // 2,
+                       "l2": "latency-bound chain; no flush",
+                       "parallelism": "dp%d" % ws if ws > 1 else "single"},
+            "fp64_grads_per_s": ws / res["fp64"]["s_per_grad"], "mixed_grads_per_s": ws / mx["s_per_grad"],
+            "speedup_vs_fp64": res["fp64"]["s_per_grad"] / mx["s_per_grad"],
+            "max_abs_dg_vs_fp64": dg, "roofline": None, "gpu_launches": mx["launches"], "clocks": mx["clocks"],
+            "cpu_baseline": cpu,
+            "e2e": {"value": ws / mx["s_per_grad"], "unit": "grads/s",
+                    "h2d_bytes_per_step": int(mol._atm.nbytes + mol._env.nbytes + mol._bas.nbytes),
+                    "d2h_bytes_per_step": int(grads[args.mode].nbytes)}}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     ws, rank, local = dist_setup()
@@ -366,7 +434,7 @@ def main():
             torch.distributed.destroy_process_group()
         return
     if args.workload != "eri":
-        (run_gemm if args.workload == "gemm" else run_lambda)(args, ws, rank, local)
+        {"gemm": run_gemm, "lambda": run_lambda, "grad": run_grad}[args.workload](args, ws, rank, local)
         if ws > 1:
             torch.distributed.destroy_process_group()
         return

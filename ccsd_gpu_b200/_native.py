@@ -30,6 +30,8 @@ SIGNATURES = {
                                                  _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "ccsd_b200_split_pack": (_c_int, [_c_int, _vp, _vp, _vp, _c_dbl, _vp, _vp, _vp, _c_dbl, _c_int, _c_int,
                                       _c_int, _c_int, _vp, _vp, _vp]),
+    "ccsd_b200_eri_ip1_contract": (_c_int, [_vp, _vp, _vp, _vp, _c_int, _vp, _vp, _c_ll, _vp, _c_int, _c_int, _vp,
+                                            _vp, _vp]),
     "ccsd_b200_tc_split_gemm": (_c_int, [_c_int, _vp, _vp, _vp, _vp, _c_int, _c_int, _c_int, _c_int, _c_int,
                                          _vp, _vp, _vp, _c_dbl, _c_dbl, _c_int, _vp, _vp, _vp]),
 }

@@ -210,16 +210,21 @@ __device__ __forceinline__ void build_g_any(const double *__restrict__ p, int di
 #undef CB_G9
 #undef CB_G
 
-enum { MODE_S2KL = 0, MODE_QSUM = 1 };
+enum { MODE_S2KL = 0, MODE_QSUM = 1, MODE_GRAD = 2 };
 
 struct S2klOut {
     double *out;
     long long nao_pair, comp_stride;
     int nao, i_base;
+    const double *gamma;     // MODE_GRAD: dense [nao]^4 density in the Cartesian AO basis
 };
 
 // Integrals of one shell quartet by one warp.  MODE_S2KL writes the s2kl block,
-// MODE_QSUM writes two checksums per component of the Cartesian quartet block.
+// MODE_QSUM writes two checksums per component of the Cartesian quartet block,
+// MODE_GRAD contracts the block with so.gamma: per component
+//   q[c] += w * sum_{ijkl in the block} I_c[ijkl] gamma[ijkl],
+// w = 1 for k shell == l shell (the full k,l block) and 2 otherwise (the
+// (l,k) half of a gamma that is symmetric in k <-> l).
 template <int D, int MODE, bool LOW>
 __device__ void eri_quartet(const int *__restrict__ atm, const int *__restrict__ bas,
                             const double *__restrict__ env, const int *__restrict__ ao_loc,
@@ -384,6 +389,32 @@ __device__ void eri_quartet(const int *__restrict__ atm, const int *__restrict__
 #pragma unroll
                     for (int c = 0; c < NC; c++) so.out[c * so.comp_stride + addr] = acc[n][c];
                 }
+            }
+        } else if (MODE == MODE_GRAD) {
+            const long long nao = so.nao;
+            const int i0 = ao_loc[ish], j0 = ao_loc[jsh], k0 = ao_loc[ksh], l0 = ao_loc[lsh];
+            double sv[NC];
+#pragma unroll
+            for (int c = 0; c < NC; c++) sv[c] = 0.0;
+#pragma unroll
+            for (int n = 0; n < GW; n++) {
+                const int f = f0 + n * FW + flane;
+                if (f < nf && grp == 0) {
+                    int t = f;
+                    const int fl = t % nfl; t /= nfl;
+                    const int fk = t % nfk; t /= nfk;
+                    const int fj = t % nfj;
+                    const int fi = t / nfj;
+                    const double gv = so.gamma[(((i0 + fi) * nao + (j0 + fj)) * nao + (k0 + fk)) * nao + (l0 + fl)];
+#pragma unroll
+                    for (int c = 0; c < NC; c++) sv[c] = fma(acc[n][c], gv, sv[c]);
+                }
+            }
+            const double wkl = ksh == lsh ? 1.0 : 2.0;
+#pragma unroll
+            for (int c = 0; c < NC; c++) {
+                for (int o = 16; o > 0; o >>= 1) sv[c] += __shfl_xor_sync(0xffffffffu, sv[c], o);
+                if (lane == 0) qsum[c] += wkl * sv[c];
             }
         } else {
 #pragma unroll
@@ -576,6 +607,23 @@ __device__ void eri_quartet_cta(const int *__restrict__ atm, const int *__restri
                            k * (k + 1) / 2 + l] = acc[n];
                 }
             }
+        } else if (MODE == MODE_GRAD) {
+            const long long nao = so.nao;
+            const int i0 = ao_loc[ish], j0 = ao_loc[jsh], k0 = ao_loc[ksh], l0 = ao_loc[lsh];
+#pragma unroll
+            for (int n = 0; n < kHeavyAcc; n++) {
+                const int e = e0 + tid + n * kHeavyThreads;
+                if (e < ne) {
+                    const int f = e / NC, c = e - f * NC;
+                    int t = f;
+                    const int fl = t % nfl; t /= nfl;
+                    const int fk = t % nfk; t /= nfk;
+                    const int fj = t % nfj;
+                    const int fi = t / nfj;
+                    qv[c] = fma(acc[n], so.gamma[(((i0 + fi) * nao + (j0 + fj)) * nao + (k0 + fk)) * nao + (l0 + fl)],
+                                qv[c]);
+                }
+            }
         } else {
 #pragma unroll
             for (int n = 0; n < kHeavyAcc; n++) {
@@ -589,18 +637,20 @@ __device__ void eri_quartet_cta(const int *__restrict__ atm, const int *__restri
         }
     }
     if (MODE != MODE_S2KL) {
+        constexpr int NOUT = MODE == MODE_QSUM ? 2 * NC : NC;
+        const double wkl = MODE == MODE_GRAD && ksh != lsh ? 2.0 : 1.0;
         __shared__ double red[kHeavyThreads / 32][6];
-        for (int c = 0; c < 2 * NC; c++)
+        for (int c = 0; c < NOUT; c++)
             for (int o = 16; o > 0; o >>= 1) qv[c] += __shfl_xor_sync(0xffffffffu, qv[c], o);
         __syncthreads();
         if ((tid & 31) == 0)
-            for (int c = 0; c < 2 * NC; c++) red[tid >> 5][c] = qv[c];
+            for (int c = 0; c < NOUT; c++) red[tid >> 5][c] = qv[c];
         __syncthreads();
         if (tid == 0)
-            for (int c = 0; c < 2 * NC; c++) {
+            for (int c = 0; c < NOUT; c++) {
                 double t = 0.0;
                 for (int w = 0; w < kHeavyThreads / 32; w++) t += red[w][c];
-                qsum[c] = t;
+                qsum[c] = wkl * t;
             }
     }
 }
@@ -642,25 +692,30 @@ __global__ void __launch_bounds__(kWarps * 32, LOW ? (D ? 2 : 3) : 2) eri_s2kl_k
     }
 }
 
-// Explicit quartet list (int4 shells), two checksums per component per quartet.
-template <int D, bool LOW>
+// Explicit quartet list (int4 shells): MODE_QSUM writes two checksums per
+// component per quartet, MODE_GRAD one gamma contraction per component.
+template <int D, bool LOW, int MODE = MODE_QSUM>
 __global__ void __launch_bounds__(kWarps * 32, LOW ? (D ? 2 : 3) : 2) eri_qsum_kernel(
     const int *__restrict__ atm, const int *__restrict__ bas, const double *__restrict__ env,
-    const int4 *__restrict__ quartets, long long nq, double *__restrict__ qsum, int smem_warp)
+    const int4 *__restrict__ quartets, long long nq, double *__restrict__ qsum, int smem_warp,
+    const int *__restrict__ ao_loc = nullptr, const double *__restrict__ gamma = nullptr, int nao = 0)
 {
     extern __shared__ double smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     double *wsm = smem + warp * smem_warp;
     S2klOut so = {};
+    so.gamma = gamma;
+    so.nao = nao;
     constexpr int NC = D ? 3 : 1;
+    constexpr int NOUT = MODE == MODE_QSUM ? 2 * NC : NC;
     for (long long q = (long long)blockIdx.x * kWarps + warp; q < nq; q += (long long)gridDim.x * kWarps) {
         const int4 s = quartets[q];
         if (quartet_nf(bas, s.x, s.y, s.z, s.w) > kHeavyNf) continue;
-        double acc[2 * NC];
-        for (int c = 0; c < 2 * NC; c++) acc[c] = 0.0;
-        eri_quartet<D, MODE_QSUM, LOW>(atm, bas, env, nullptr, s.x, s.y, s.z, s.w, wsm, smem_warp, so, acc, lane);
+        double acc[NOUT];
+        for (int c = 0; c < NOUT; c++) acc[c] = 0.0;
+        eri_quartet<D, MODE, LOW>(atm, bas, env, ao_loc, s.x, s.y, s.z, s.w, wsm, smem_warp, so, acc, lane);
         if (lane == 0)
-            for (int c = 0; c < 2 * NC; c++) qsum[q * 2 * NC + c] = acc[c];
+            for (int c = 0; c < NOUT; c++) qsum[q * NOUT + c] = acc[c];
     }
 }
 
@@ -685,20 +740,44 @@ __global__ void __launch_bounds__(kHeavyThreads, 1) eri_s2kl_heavy_kernel(
 }
 
 // Heavy quartets of an explicit list (light ones are skipped here).
-template <int D, bool LOW>
+template <int D, bool LOW, int MODE = MODE_QSUM>
 __global__ void __launch_bounds__(kHeavyThreads, 1) eri_qsum_heavy_kernel(
     const int *__restrict__ atm, const int *__restrict__ bas, const double *__restrict__ env,
-    const int4 *__restrict__ quartets, long long nq, double *__restrict__ qsum, int smem_doubles)
+    const int4 *__restrict__ quartets, long long nq, double *__restrict__ qsum, int smem_doubles,
+    const int *__restrict__ ao_loc = nullptr, const double *__restrict__ gamma = nullptr, int nao = 0)
 {
     extern __shared__ double smem[];
     S2klOut so = {};
+    so.gamma = gamma;
+    so.nao = nao;
     constexpr int NC = D ? 3 : 1;
+    constexpr int NOUT = MODE == MODE_QSUM ? 2 * NC : NC;
     for (long long q = blockIdx.x; q < nq; q += gridDim.x) {
         const int4 s = quartets[q];
         if (quartet_nf(bas, s.x, s.y, s.z, s.w) <= kHeavyNf) continue;
-        eri_quartet_cta<D, MODE_QSUM, LOW>(atm, bas, env, nullptr, s.x, s.y, s.z, s.w, smem, smem_doubles, so,
-                                           qsum + q * 2 * NC);
+        eri_quartet_cta<D, MODE, LOW>(atm, bas, env, ao_loc, s.x, s.y, s.z, s.w, smem, smem_doubles, so,
+                                      qsum + q * NOUT);
     }
+}
+
+// out[s][c] = sum over quartets q in [seg[s], seg[s+1]) of qv[q][c], c < 3,
+// summed in a fixed order (one CTA per segment, fixed-shape tree).
+__global__ void segment_sum3_kernel(const double *__restrict__ qv, const long long *__restrict__ seg,
+                                    double *__restrict__ out)
+{
+    __shared__ double red[3][256];
+    const int s = blockIdx.x, tid = threadIdx.x;
+    double a[3] = {0.0, 0.0, 0.0};
+    for (long long q = seg[s] + tid; q < seg[s + 1]; q += 256)
+        for (int c = 0; c < 3; c++) a[c] += qv[q * 3 + c];
+    for (int c = 0; c < 3; c++) red[c][tid] = a[c];
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+        if (tid < h)
+            for (int c = 0; c < 3; c++) red[c][tid] += red[c][tid + h];
+        __syncthreads();
+    }
+    if (tid < 3) out[s * 3 + tid] = red[tid][0];
 }
 
 // ---- Cartesian -> spherical transform of an s2kl block (two passes) ----
@@ -941,6 +1020,53 @@ int ccsd_b200_eri_quartet_checksums(int deriv, const int32_t *atm, const int32_t
 #undef CB_LAUNCH_QSUM
     cudaStreamWaitEvent(st, aux->join, 0);
     return check_launch("eri_qsum_kernel");
+}
+
+int ccsd_b200_eri_ip1_contract(const int32_t *atm, const int32_t *bas, const double *env, const int32_t *ao_loc,
+                               int nao, const double *gamma, const int32_t *quartets, long long nq,
+                               const long long *seg, int nseg, int lmax, double *qwork, double *out, void *stream)
+{
+    if (!atm || !bas || !env || !ao_loc || nao <= 0 || !gamma || !quartets || nq < 0 || !seg || nseg <= 0 ||
+        lmax < 0 || !qwork || !out) {
+        set_error("ccsd_b200_eri_ip1_contract: invalid argument");
+        return CCSD_B200_ERR_ARG;
+    }
+    if (lmax > CB_LMAX) {
+        set_error("ccsd_b200_eri_ip1_contract: l = %d > %d is not supported", lmax, CB_LMAX);
+        return CCSD_B200_ERR_UNSUPPORTED;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc;
+    if (nq > 0) {
+        const int sw = smem_per_warp(lmax, 1);
+        const size_t smem = (size_t)sw * kWarps * sizeof(double);
+        long long grid = (nq + kWarps - 1) / kWarps;
+        const long long gmax = (long long)num_sms() * 16;
+        if (grid > gmax) grid = gmax;
+        const int4 *q4 = reinterpret_cast<const int4 *>(quartets);
+        AuxStream *aux = nullptr;
+        if ((rc = aux_stream(&aux))) return rc;
+        cudaEventRecord(aux->fork, st);
+        cudaStreamWaitEvent(aux->s, aux->fork, 0);
+        const int hd = heavy_smem_doubles(lmax, 1);
+        const size_t hsmem = (size_t)hd * sizeof(double);
+        const long long hg = nq < (long long)num_sms() ? nq : (long long)num_sms();
+#define CB_LAUNCH_GRAD(LOWV)                                                                                      \
+    if ((rc = prepare_kernel(eri_qsum_heavy_kernel<1, LOWV, MODE_GRAD>, hsmem))) return rc;                       \
+    eri_qsum_heavy_kernel<1, LOWV, MODE_GRAD><<<(int)hg, kHeavyThreads, hsmem, aux->s>>>(atm, bas, env, q4, nq,   \
+                                                                                      qwork, hd, ao_loc, gamma, nao); \
+    if ((rc = check_launch("eri_qsum_heavy_kernel<grad>"))) return rc;                                            \
+    cudaEventRecord(aux->join, aux->s);                                                                            \
+    if ((rc = prepare_kernel(eri_qsum_kernel<1, LOWV, MODE_GRAD>, smem))) return rc;                              \
+    eri_qsum_kernel<1, LOWV, MODE_GRAD><<<(int)grid, kWarps * 32, smem, st>>>(atm, bas, env, q4, nq, qwork, sw,     \
+                                                                            ao_loc, gamma, nao);
+        if (lmax <= 2) { CB_LAUNCH_GRAD(true) } else { CB_LAUNCH_GRAD(false) }
+#undef CB_LAUNCH_GRAD
+        cudaStreamWaitEvent(st, aux->join, 0);
+        if ((rc = check_launch("eri_qsum_kernel<grad>"))) return rc;
+    }
+    segment_sum3_kernel<<<nseg, 256, 0, st>>>(qwork, seg, out);
+    return check_launch("segment_sum3_kernel");
 }
 
 int ccsd_b200_cart2sph_s2kl(const double *cart, double *tmp, double *out, int ncomp, int nfc, int naoc, int nfs,

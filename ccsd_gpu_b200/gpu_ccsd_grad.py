@@ -9,10 +9,14 @@ numpy arrays like the reference.  Everything runs on the device:
   * RDM intermediates through the contraction engine in the CC object's
     precision; MO->AO transform, all gradient contractions, the CPHF
     (Z-vector) solve and the one-electron terms in FP64;
-  * two-electron derivative integrals from ``compute_int2e_ip1_gpu`` per atom
-    block (the reference falls back to CPU libcint below nao = 50), Imat from
-    the SCF's resident ERIs, one-electron derivative integrals from the
-    ``int1e`` kernel (the reference uses CPU libcint through PySCF);
+  * the two-electron gradient term: the 2-RDM and the P x relaxed-density
+    products (the reference's de_k and vhf1 terms) form one density that is
+    contracted with int2e_ip1 inside the ERI kernel, shell quartet by shell
+    quartet (:func:`ccsd_gpu_b200.cuda.ip1_contract.contract_int2e_ip1`); no
+    derivative integral is stored (the reference stores each atom block and
+    falls back to CPU libcint below nao = 50).  Imat comes from the SCF's
+    resident ERIs, one-electron derivative integrals from the ``int1e``
+    kernel (the reference uses CPU libcint through PySCF);
   * the Z-vector equations (e_a - e_i) x + A x = -Xvo are solved directly in
     FP64 (the reference iterates PySCF's cphf.solve to 1e-9).
 ``CCSDEnergy`` wraps E(R) in a torch.autograd.Function whose backward is
@@ -23,7 +27,7 @@ import torch
 
 from . import _native
 from .contract import contract
-from .cuda.int2e_ip1_gpu import compute_int2e_ip1_gpu
+from .cuda.ip1_contract import contract_int2e_ip1
 from .int1e import intor1e
 
 
@@ -173,14 +177,6 @@ def _rdm2_mo2ao_gpu(mycc, d2, mo_coeff):
     return dm2.reshape(nao * nao, nao * nao)[p[:, None], p[None, :]]
 
 
-def _unpack_kl(s2kl, nao):
-    k, l = torch.tril_indices(nao, nao, device=s2kl.device)
-    full = torch.empty(s2kl.shape[:-1] + (nao, nao), dtype=torch.float64, device=s2kl.device)
-    full[..., k, l] = s2kl
-    full[..., l, k] = s2kl
-    return full
-
-
 def grad_elec_gpu(mycc, t1, t2, l1, l2, atmlst=None, verbose=None):
     """Electronic part of the CCSD gradient, numpy (natm, 3)
     (ref: ccsd_gpu/gpu_ccsd_grad.py:344-586)."""
@@ -202,21 +198,7 @@ def grad_elec_gpu(mycc, t1, t2, l1, l2, atmlst=None, verbose=None):
     atmlst = range(mol.natm) if atmlst is None else atmlst
     off = mol.offset_nr_by_atom()
     de = torch.zeros((mol.natm, 3), dtype=torch.float64, device=dev)
-    vhf1 = torch.zeros((mol.natm, 3, nao, nao), dtype=torch.float64, device=dev)
     Imat = 0.5 * torch.einsum("ipkl,iqkl->pq", eri, dm2)
-    for a in atmlst:
-        s0, s1_, p0, p1 = (int(v) for v in off[a])
-        if s1_ <= s0:
-            continue
-        I = _unpack_kl(compute_int2e_ip1_gpu(mol, s0, s1_), nao)          # (3, nf, nao, nao, nao)
-        de[a] -= torch.einsum("xijkl,ijkl->x", I, dm2[p0:p1])
-        v = torch.einsum("xijkl,ij->xkl", I, P[p0:p1])
-        v -= 0.5 * torch.einsum("xijkl,il->xkj", I, P[p0:p1])
-        v[:, p0:p1] += torch.einsum("xijkl,kl->xij", I, P)
-        v[:, p0:p1] -= 0.5 * torch.einsum("xijkl,jk->xil", I, P)
-        vhf1[a] = v
-        del I
-    del dm2
     S = mf.get_ovlp()
     Imat = -(C.T @ Imat @ S @ C)
     dm1mo = torch.zeros((nmo, nmo), dtype=torch.float64, device=dev)
@@ -242,6 +224,18 @@ def grad_elec_gpu(mycc, t1, t2, l1, l2, atmlst=None, verbose=None):
     dm1p = P + 2 * dm1
     dm1 = dm1 + P
     zeta = zeta + (Co * (2 * e[:nocc])) @ Co.T
+    # Two-electron term: the 2-RDM and the HF-like products of P with the
+    # relaxed density (ref: ccsd_gpu/gpu_ccsd_grad.py:416-500, de_k and vhf1)
+    # in one density, symmetrised in k <-> l, contracted with int2e_ip1 that
+    # is recomputed shell quartet by shell quartet and never stored.
+    gam = dm2
+    del dm2
+    gam += P[:, :, None, None] * dm1p[None, None] + dm1p[:, :, None, None] * P[None, None]
+    gam -= 0.5 * torch.einsum("il,kj->ijkl", P, dm1p)
+    gam -= 0.5 * torch.einsum("jk,il->ijkl", P, dm1p)
+    gam = 0.5 * (gam + gam.permute(0, 1, 3, 2))
+    de -= contract_int2e_ip1(mol, gam)
+    del gam
     charges = mol.atom_charges()
     for a in atmlst:
         _, _, p0, p1_ = (int(v) for v in off[a])
@@ -255,7 +249,6 @@ def grad_elec_gpu(mycc, t1, t2, l1, l2, atmlst=None, verbose=None):
         de[a] -= torch.einsum("xij,ij->x", s1a, zeta[p0:p1_])
         de[a] -= torch.einsum("xji,ij->x", s1a, zeta[:, p0:p1_])
         de[a] -= 2 * torch.einsum("xij,ij->x", s1a, vhf_s1occ[p0:p1_])
-        de[a] -= torch.einsum("xij,ij->x", vhf1[a], dm1p)
     return de[list(atmlst)].cpu().numpy()
 
 

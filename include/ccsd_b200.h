@@ -122,6 +122,25 @@ int ccsd_b200_int1e_cart(int op, const int32_t *atm, int natm, const int32_t *ba
 int ccsd_b200_fp64_fma_probe(double *out, int blocks, int iters, void *stream);
 
 /*
+ * Two-electron part of the nuclear gradient without storing ERI derivatives:
+ * for every shell quartet q = (I, J, K, L) of `quartets` (decontracted shells,
+ * K >= L, derivative on I) the (dI J|K L) block is built shell quartet by shell
+ * quartet and contracted at once with the density `gamma`,
+ *   qwork[q][x] = w_q * sum_{ijkl in q} (d/dx_i ij|kl) gamma[i][j][k][l],
+ * w_q = 1 if K == L else 2 (gamma must be symmetric in k <-> l; dense
+ * [nao]^4, FP64, in the Cartesian AO basis of ao_loc).  Then
+ *   out[s][x] = sum_{q in [seg[s], seg[s+1])} qwork[q][x]
+ * in a fixed order (list sorted by the atom of I gives per-atom gradients).
+ * qwork holds nq * 3 doubles, out nseg * 3.  Replaces the int2e_ip1 -> Gamma
+ * contraction loop of the Phase-3 gradient, which stores the derivative
+ * integrals of each atom block (ref: ccsd_gpu/gpu_ccsd_grad.py:416-500,
+ * ccsd_gpu/cuda/int2e_ip1_gpu.py:148-330).
+ */
+int ccsd_b200_eri_ip1_contract(const int32_t *atm, const int32_t *bas, const double *env, const int32_t *ao_loc,
+                               int nao, const double *gamma, const int32_t *quartets, long long nq,
+                               const long long *seg, int nseg, int lmax, double *qwork, double *out, void *stream);
+
+/*
  * Split-precision tensor-core contraction, step 1: gather + split.
  *   v[r][k] = c1 * src1[o1r[r] + o1k[k]] + c2 * src2[o2r[r] + o2k[k]]   (src2 may be NULL)
  * for r < rows, k < K (zero elsewhere), written as hi + lo parts, K-major,
