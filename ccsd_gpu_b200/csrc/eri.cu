@@ -441,6 +441,496 @@ __device__ void eri_quartet(const int *__restrict__ atm, const int *__restrict__
     }
 }
 
+// ===========================================================================
+// Contracted-HRR path for l <= 2 quartets (one warp per quartet).
+//
+// The warp path above applies both horizontal recurrences (HRR) to the 2D
+// tables of every slot and forms every output of the block per slot.  For
+// contracted shells (many primitive quartets x roots) it is cheaper to
+// accumulate the vertical/transfer-recurrence integrals
+//     [e|f] = sum_slots Ix(ex,fx) Iy(ey,fy) Iz(ez,fz),  |e| = A0..A0+lj,
+//                                                       |f| = lk..lk+ll,
+// over all slots (registers, lane-owned) and to run the HRR once, in 6D, on
+// the contracted [e|f]:
+//     (e|c, d+1_x) = (e|c+1_x, d) + CD_x (e|c, d)        (ket, per e row)
+//     (a, b+1_x|   = (a+1_x, b|   + AB_x (a, b|         (bra, per (c,d) column)
+// int2e uses one set with A0 = li.  int2e_ip1 uses two: A0 = li + 1 with the
+// factor 2 a_i folded into each slot, and A0 = li - 1; the derivative is
+//     d/dx_i (ij|kl) = i_x (i-1_x j|kl) - 2 a_i (i+1_x j|kl).
+// Per slot this is 3 loads + 3 flops per [e|f] value instead of ~9 loads and
+// ~15 flops per output and component, and the recurrences run once per batch
+// instead of once per 256-output chunk.
+// ===========================================================================
+static constexpr int kHcMaxJ = 40;      // accumulators per lane (<= 1280 per quartet)
+static constexpr int kHcSmem = 3072;    // doubles of shared memory per warp on this path
+
+__host__ __device__ constexpr int hc_ncart(int l) { return (l + 1) * (l + 2) / 2; }
+__host__ __device__ constexpr int hc_csum(int l0, int l1)
+{
+    int s = 0;
+    for (int l = l0; l <= l1; l++) s += hc_ncart(l);
+    return s;
+}
+// Cartesian component k of shell l (order xx, xy, xz, yy, yz, zz, ...)
+__host__ __device__ constexpr int hc_n(int k)
+{
+    int n = 0;
+    while ((n + 1) * (n + 2) / 2 <= k) n++;
+    return n;
+}
+__host__ __device__ constexpr int hc_lx(int l, int k) { return l - hc_n(k); }
+__host__ __device__ constexpr int hc_lz(int k) { return k - hc_n(k) * (hc_n(k) + 1) / 2; }
+__host__ __device__ constexpr int hc_ly(int l, int k) { return hc_n(k) - hc_lz(k); }
+__host__ __device__ constexpr int hc_idx(int lx, int ly, int lz) { return (ly + lz) * (ly + lz + 1) / 2 + lz; }
+// index in shell l+1 of component k of shell l raised by one in direction x
+__host__ __device__ constexpr int hc_up(int l, int k, int x)
+{
+    return hc_idx(hc_lx(l, k) + (x == 0), hc_ly(l, k) + (x == 1), hc_lz(k) + (x == 2));
+}
+
+// 2D vertical + transfer recurrences of one (slot, direction), no HRR:
+// g[e + f * (LE + 1)], e <= LE, f <= LF.
+template <int LE, int LF>
+__device__ __noinline__ void hc_build_2d(const double *__restrict__ p, int dir, double *__restrict__ g)
+{
+    const double c00 = p[dir], c01 = p[3 + dir], b00 = p[6], b10 = p[7], b01 = p[8];
+    double prev[LE + 1], cur[LE + 1];
+    cur[0] = dir == 0 ? p[9] : 1.0;
+#pragma unroll
+    for (int n = 0; n < LE; n++) cur[n + 1] = c00 * cur[n] + (n ? n * b10 * cur[n - 1] : 0.0);
+#pragma unroll
+    for (int n = 0; n <= LE; n++) prev[n] = 0.0;
+#pragma unroll
+    for (int m = 0; m <= LF; m++) {
+#pragma unroll
+        for (int n = 0; n <= LE; n++) g[n + m * (LE + 1)] = cur[n];
+        if (m < LF) {
+            double nxt[LE + 1];
+#pragma unroll
+            for (int n = 0; n <= LE; n++)
+                nxt[n] = c01 * cur[n] + (m ? m * b01 * prev[n] : 0.0) + (n ? n * b00 * cur[n - 1] : 0.0);
+#pragma unroll
+            for (int n = 0; n <= LE; n++) {
+                prev[n] = cur[n];
+                cur[n] = nxt[n];
+            }
+        }
+    }
+}
+
+#define CB_B2(c) case c: hc_build_2d<(c) / 5, (c) % 5>(p, dir, g); return;
+__device__ __forceinline__ void hc_build_any(const double *__restrict__ p, int dir, int le, int lf,
+                                             double *__restrict__ g)
+{
+    switch (le * 5 + lf) {
+        CB_B2(0) CB_B2(1) CB_B2(2) CB_B2(3) CB_B2(4) CB_B2(5) CB_B2(6) CB_B2(7) CB_B2(8) CB_B2(9)
+        CB_B2(10) CB_B2(11) CB_B2(12) CB_B2(13) CB_B2(14) CB_B2(15) CB_B2(16) CB_B2(17) CB_B2(18) CB_B2(19)
+        CB_B2(20) CB_B2(21) CB_B2(22) CB_B2(23) CB_B2(24) CB_B2(25) CB_B2(26) CB_B2(27) CB_B2(28) CB_B2(29)
+        default: break;
+    }
+}
+#undef CB_B2
+
+// One line of the 6D HRR in registers: in[s * istride], s over the components
+// of shells L0..L0+L1 (shell-major), -> out[(a * ncart(L1) + b) * ostride],
+// (a, b+1_x) = (a+1_x, b) + R_x (a, b).  L1 <= 2.
+template <int L0, int L1>
+__device__ __noinline__ void hc_hrr_line(const double *__restrict__ in, int istride, double *__restrict__ out,
+                                         int ostride, double rx, double ry, double rz)
+{
+    constexpr int N0 = hc_csum(L0, L0 + L1);
+    constexpr int NA = hc_ncart(L0);
+    double v0[N0];
+#pragma unroll
+    for (int s = 0; s < N0; s++) v0[s] = in[s * istride];
+    if constexpr (L1 == 0) {
+#pragma unroll
+        for (int a = 0; a < NA; a++) out[a * ostride] = v0[a];
+    } else {
+        const double R[3] = {rx, ry, rz};
+        // level 1: (a, 1_x) for |a| = L0 .. L0+L1-1, stored v1[x][a-flat]
+        constexpr int N1 = hc_csum(L0, L0 + L1 - 1);
+        double v1[3][N1];
+#pragma unroll
+        for (int x = 0; x < 3; x++) {
+            int off = 0, offu = NA;        // start of shell A (flat) and of shell A+1 in v0
+#pragma unroll
+            for (int A = L0; A < L0 + L1; A++) {
+#pragma unroll
+                for (int k = 0; k < hc_ncart(A); k++)
+                    v1[x][off + k] = v0[offu + hc_up(A, k, x)] + R[x] * v0[off + k];
+                off += hc_ncart(A);
+                offu += hc_ncart(A + 1);
+            }
+        }
+        if constexpr (L1 == 1) {
+#pragma unroll
+            for (int a = 0; a < NA; a++)
+#pragma unroll
+                for (int x = 0; x < 3; x++) out[(a * 3 + x) * ostride] = v1[x][a];
+        } else {
+            // level 2: b in (xx, xy, xz, yy, yz, zz); first raised direction x,
+            // b - 1_x in level 1 as direction y
+            constexpr int bx[6] = {0, 0, 0, 1, 1, 2};     // direction peeled off
+            constexpr int by[6] = {0, 1, 2, 1, 2, 2};     // level-1 direction left
+#pragma unroll
+            for (int a = 0; a < NA; a++)
+#pragma unroll
+                for (int b = 0; b < 6; b++)
+                    out[(a * 6 + b) * ostride] = v1[by[b]][NA + hc_up(L0, a, bx[b])] + R[bx[b]] * v1[by[b]][a];
+        }
+    }
+}
+
+#define CB_H(c) case c: hc_hrr_line<(c) / 3, (c) % 3>(in, istride, out, ostride, rx, ry, rz); return;
+__device__ __forceinline__ void hc_hrr_any(int l0, int l1, const double *__restrict__ in, int istride,
+                                           double *__restrict__ out, int ostride, double rx, double ry, double rz)
+{
+    switch (l0 * 3 + l1) {
+        CB_H(0) CB_H(1) CB_H(2) CB_H(3) CB_H(4) CB_H(5) CB_H(6) CB_H(7) CB_H(8) CB_H(9) CB_H(10) CB_H(11)
+        default: break;
+    }
+}
+#undef CB_H
+
+// Layout of one quartet on this path; hc_plan() decides whether it applies.
+// The quartet may be computed as (ij|lk) (kswap: the larger ket shell carries
+// the recurrences) or, for int2e, as (ji|kl) (bswap); outputs are mapped back.
+struct HcPlan {
+    int nset, a0[2], ne[2], nf_ket, nacc, setoff[2];
+    int nc, nd, ncd, na[2], nb, rowoff[2], nrows, braoff[2], nbra, nket;
+    bool kswap, bswap;
+};
+
+__device__ __forceinline__ bool hc_plan(int D, int li, int lj, int lk, int ll, HcPlan &h,
+                                        int maxacc = 32 * kHcMaxJ, int cap = kHcSmem, bool always = false)
+{
+    if (li > 2 || lj > 2 || lk > 2 || ll > 2) return false;
+    h.kswap = lk < ll;
+    h.bswap = D == 0 && li < lj;
+    if (h.kswap) { const int t = lk; lk = ll; ll = t; }
+    if (h.bswap) { const int t = li; li = lj; lj = t; }
+    h.nset = D ? (li > 0 ? 2 : 1) : 1;
+    h.a0[0] = D ? li + 1 : li;
+    h.a0[1] = li - 1;
+    h.nf_ket = hc_csum(lk, lk + ll);
+    h.nc = hc_ncart(lk);
+    h.nd = hc_ncart(ll);
+    h.ncd = h.nc * h.nd;
+    h.nb = hc_ncart(lj);
+    h.nacc = 0;
+    h.nrows = 0;
+    h.nbra = 0;
+    for (int s = 0; s < h.nset; s++) {
+        h.ne[s] = hc_csum(h.a0[s], h.a0[s] + lj);
+        h.na[s] = hc_ncart(h.a0[s]);
+        h.setoff[s] = h.nacc;
+        h.nacc += h.ne[s] * h.nf_ket;
+        h.rowoff[s] = h.nrows;
+        h.nrows += h.ne[s];
+        h.braoff[s] = h.nbra;
+        h.nbra += h.na[s] * h.nb;
+    }
+    h.nket = h.nrows * h.ncd;
+    const int nf = hc_ncart(li) * h.nb * h.ncd;
+    const int lo = h.nacc > h.nbra * h.ncd ? h.nacc : h.nbra * h.ncd;
+    if (h.nacc > maxacc || lo + h.nket > cap) return false;
+    if (always) return true;
+    // measured: worth it when the per-output path would recompute the slots
+    // for several 256-output chunks, or when [e|f] is clearly smaller than
+    // the output block and the ket has no s shell
+    return nf > 256 || (ll > 0 && 100 * h.nacc <= 62 * nf * (D ? 3 : 1));
+}
+
+template <int NT>
+__device__ __forceinline__ void grp_sync()
+{
+    if (NT == 32) __syncwarp();
+    else __syncthreads();
+}
+
+// NT cooperating threads (a warp, or a 256-thread CTA for heavy quartets),
+// `cap` doubles of shared memory at wsm; `qsum` is added to (warp) or
+// assigned (CTA) in the checksum and gradient modes.
+template <int D, int MODE, int NJ, int NT>
+__device__ void eri_quartet_hc(const int *__restrict__ atm, const int *__restrict__ bas,
+                               const double *__restrict__ env, const int *__restrict__ ao_loc, int ish, int jsh,
+                               int ksh, int lsh, const HcPlan &h, double *__restrict__ wsm, const S2klOut &so,
+                               double *__restrict__ qsum, int lane, int cap)
+{
+    constexpr int NC = D ? 3 : 1;
+    const Shell si = load_shell(atm, bas, env, h.bswap ? jsh : ish), sj_ = load_shell(atm, bas, env, h.bswap ? ish : jsh);
+    const Shell sk_ = load_shell(atm, bas, env, h.kswap ? lsh : ksh), sl_ = load_shell(atm, bas, env, h.kswap ? ksh : lsh);
+    const int li = si.l, lj = sj_.l, lk = sk_.l, ll = sl_.l;      // computed orientation
+    const int le = li + lj + D, lf = lk + ll, s2 = (le + 1) * (lf + 1);
+    const int nroots = (li + lj + lk + ll + D) / 2 + 1;
+    const int npq = si.np * sj_.np * sk_.np * sl_.np;
+    const int nslot = npq * nroots;
+    int ns = cap / (3 * s2 + kParStride);
+    ns = ns > kMaxSlots ? kMaxSlots : ns;
+    double *par = wsm;
+    double *gbuf = wsm + ns * kParStride;
+    double AB[3], CD[3];
+    for (int x = 0; x < 3; x++) {
+        AB[x] = si.R[x] - sj_.R[x];
+        CD[x] = sk_.R[x] - sl_.R[x];
+    }
+    const double rab2 = AB[0] * AB[0] + AB[1] * AB[1] + AB[2] * AB[2];
+    const double rcd2 = CD[0] * CD[0] + CD[1] * CD[1] + CD[2] * CD[2];
+    const double pref0 = 34.986836655249725693 * common_fac(li) * common_fac(lj) * common_fac(lk) *
+                         common_fac(ll);
+
+    // lane-owned accumulators: flat t = lane + 32 j = setoff[s] + ie * nf_ket + if
+    int idx[NJ];
+    double acc[NJ];
+    const int nj = (h.nacc - lane + NT - 1) / NT;
+#pragma unroll
+    for (int j = 0; j < NJ; j++) {
+        acc[j] = 0.0;
+        idx[j] = 0;
+        const int t = lane + NT * j;
+        if (t < h.nacc) {
+            const int s = (h.nset > 1 && t >= h.setoff[1]) ? 1 : 0;
+            const int r = t - h.setoff[s];
+            int ie = r / h.nf_ket, jf = r - ie * h.nf_ket;
+            int E = h.a0[s];
+            while (ie >= hc_ncart(E)) { ie -= hc_ncart(E); E++; }
+            int F = lk;
+            while (jf >= hc_ncart(F)) { jf -= hc_ncart(F); F++; }
+            const int ex = hc_lx(E, ie), ey = hc_ly(E, ie), ez = hc_lz(ie);
+            const int fx = hc_lx(F, jf), fy = hc_ly(F, jf), fz = hc_lz(jf);
+            idx[j] = (ex + fx * (le + 1)) | ((ey + fy * (le + 1)) << 8) | ((ez + fz * (le + 1)) << 16) |
+                     ((D && s == 0) ? (1 << 24) : 0);
+        }
+    }
+    for (int s0 = 0; s0 < nslot; s0 += ns) {
+        const int s1 = min(nslot, s0 + ns);
+        grp_sync<NT>();
+        // ---- phase A: primitive-quartet data and Rys nodes/weights (as in eri_quartet)
+        const int pq0 = s0 / nroots, pq1 = (s1 - 1) / nroots + 1;
+        for (int pq = pq0 + lane; pq < pq1; pq += NT) {
+            int t = pq;
+            const int lp = t % sl_.np; t /= sl_.np;
+            const int kp = t % sk_.np; t /= sk_.np;
+            const int jp = t % sj_.np;
+            const int ip = t / sj_.np;
+            const double ai = si.exps[ip], aj = sj_.exps[jp], ak = sk_.exps[kp], al = sl_.exps[lp];
+            const double aij = ai + aj, akl = ak + al, aijkl = aij + akl;
+            double PA[3], QC[3], PQ[3];
+            for (int x = 0; x < 3; x++) {
+                PA[x] = -aj / aij * AB[x];
+                QC[x] = -al / akl * CD[x];
+                PQ[x] = (si.R[x] + PA[x]) - (sk_.R[x] + QC[x]);
+            }
+            const double rpq2 = PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2];
+            const double T = aij * akl / aijkl * rpq2;
+            const double pref = pref0 * si.coefs[ip] * sj_.coefs[jp] * sk_.coefs[kp] * sl_.coefs[lp] *
+                                exp(-ai * aj / aij * rab2 - ak * al / akl * rcd2) / (aij * akl * sqrt(aijkl));
+            double u[RYS_NROOTS_MAX], w[RYS_NROOTS_MAX];
+            rys_roots(nroots, T, u, w);
+            for (int r = 0; r < nroots; r++) {
+                const int s = pq * nroots + r;
+                if (s < s0 || s >= s1) continue;
+                double *p = par + (s - s0) * kParStride;
+                const double ua = u[r] / aijkl;
+                for (int x = 0; x < 3; x++) {
+                    p[x] = PA[x] - ua * akl * PQ[x];
+                    p[3 + x] = QC[x] + ua * aij * PQ[x];
+                }
+                p[6] = 0.5 * ua;
+                p[7] = 0.5 / aij * (1.0 - ua * akl);
+                p[8] = 0.5 / akl * (1.0 - ua * aij);
+                p[9] = w[r] * pref;
+                p[10] = 2.0 * ai;
+            }
+        }
+        grp_sync<NT>();
+        // ---- phase B: 2D tables, one (slot, direction) per lane
+        for (int it = lane; it < (s1 - s0) * 3; it += NT) {
+            const int s = it / 3, dir = it - s * 3;
+            hc_build_any(par + s * kParStride, dir, le, lf, gbuf + (s * 3 + dir) * s2);
+        }
+        grp_sync<NT>();
+        // ---- phase C: [e|f] += Ix Iy Iz (x 2 a_i on the raised set)
+        for (int s = 0; s < s1 - s0; s++) {
+            const double *gx = gbuf + s * 3 * s2, *gy = gx + s2, *gz = gy + s2;
+            const double a2 = par[s * kParStride + 10];
+#pragma unroll
+            for (int j = 0; j < NJ; j++) {
+                if (j < nj) {
+                    const int o = idx[j];
+                    const double v = gx[o & 255] * gy[(o >> 8) & 255];
+                    acc[j] = fma(v * gz[(o >> 16) & 255], (o >> 24) ? a2 : 1.0, acc[j]);
+                }
+            }
+        }
+    }
+    // ---- contracted HRR.  Shared memory: [e|f] at [0, nacc), ket rows at the
+    // top [cap - nket, cap), bra results at [0, nbra * ncd).
+    grp_sync<NT>();
+#pragma unroll
+    for (int j = 0; j < NJ; j++)
+        if (j < nj) wsm[lane + NT * j] = acc[j];
+    grp_sync<NT>();
+    double *ket = wsm + (cap - h.nket);
+    for (int row = lane; row < h.nrows; row += NT) {
+        const int s = (h.nset > 1 && row >= h.rowoff[1]) ? 1 : 0;
+        const int ie = row - h.rowoff[s];
+        hc_hrr_any(lk, ll, wsm + h.setoff[s] + ie * h.nf_ket, 1, ket + row * h.ncd, 1, CD[0], CD[1], CD[2]);
+    }
+    grp_sync<NT>();
+    double *bra = wsm;
+    for (int col = lane; col < h.nset * h.ncd; col += NT) {
+        const int s = col / h.ncd, cd = col - s * h.ncd;
+        hc_hrr_any(h.a0[s], lj, ket + h.rowoff[s] * h.ncd + cd, h.ncd, bra + h.braoff[s] * h.ncd + cd, h.ncd,
+                   AB[0], AB[1], AB[2]);
+    }
+    grp_sync<NT>();
+    // ---- outputs (fi, fj, fk, fl) x component, then the MODE epilogue
+    const int nfi = hc_ncart(li), nfj = h.nb, nfk = h.nc, nfl = h.nd;      // computed orientation
+    const int nf = nfi * nfj * h.ncd;
+    const int onj = h.bswap ? nfi : nfj, onk = h.kswap ? nfl : nfk, onl = h.kswap ? nfk : nfl;   // original
+    double r1[NC], r2[NC];
+#pragma unroll
+    for (int c = 0; c < NC; c++) r1[c] = r2[c] = 0.0;
+    for (int f = lane; f < nf; f += NT) {
+        const int cd = f % h.ncd;
+        const int fij = f / h.ncd;
+        const int fj = fij % nfj, fi = fij / nfj;
+        double v[NC];
+        if (D == 0) {
+            v[0] = bra[(fi * nfj + fj) * h.ncd + cd];
+        } else {
+            const int ix = hc_lx(li, fi), iy = hc_ly(li, fi), iz = hc_lz(fi);
+            const int ie[3] = {ix, iy, iz};
+#pragma unroll
+            for (int x = 0; x < NC; x++) {
+                const int up = hc_up(li, fi, x);
+                double t = -bra[(h.braoff[0] + up * nfj + fj) * h.ncd + cd];
+                if (ie[x] > 0) {
+                    const int dn = hc_idx(ix - (x == 0), iy - (x == 1), iz - (x == 2));
+                    t = fma((double)ie[x], bra[(h.braoff[1] + dn * nfj + fj) * h.ncd + cd], t);
+                }
+                v[x] = t;
+            }
+        }
+        // back to the original shell order
+        int fk = cd / nfl, fl = cd - fk * nfl;
+        if (h.kswap) { const int t = fk; fk = fl; fl = t; }
+        const int oi = h.bswap ? fj : fi, oj = h.bswap ? fi : fj;
+        if (MODE == MODE_S2KL) {
+            if (ksh == lsh && fl > fk) continue;
+            const int i0 = ao_loc[ish] - so.i_base, j0 = ao_loc[jsh], k0 = ao_loc[ksh], l0 = ao_loc[lsh];
+            const long long k = k0 + fk, l = l0 + fl;
+            const long long addr = ((long long)(i0 + oi) * so.nao + (j0 + oj)) * so.nao_pair + k * (k + 1) / 2 + l;
+#pragma unroll
+            for (int c = 0; c < NC; c++) so.out[c * so.comp_stride + addr] = v[c];
+        } else if (MODE == MODE_GRAD) {
+            const long long nao = so.nao;
+            const int i0 = ao_loc[ish], j0 = ao_loc[jsh], k0 = ao_loc[ksh], l0 = ao_loc[lsh];
+            const double gv = so.gamma[(((i0 + oi) * nao + (j0 + oj)) * nao + (k0 + fk)) * nao + (l0 + fl)];
+#pragma unroll
+            for (int c = 0; c < NC; c++) r1[c] = fma(v[c], gv, r1[c]);
+        } else {
+            // checksum weights follow the original (fi, fj, fk, fl) row-major function index
+            const int fr = ((oi * onj + oj) * onk + fk) * onl + fl;
+#pragma unroll
+            for (int c = 0; c < NC; c++) {
+                r1[c] += v[c] * (1.0 + 0.125 * (fr & 7));
+                r2[c] += v[c] * v[c];
+            }
+        }
+    }
+    if (MODE != MODE_S2KL) {
+        const double wkl = MODE == MODE_GRAD && ksh != lsh ? 2.0 : 1.0;
+#pragma unroll
+        for (int c = 0; c < NC; c++)
+            for (int o = 16; o > 0; o >>= 1) {
+                r1[c] += __shfl_xor_sync(0xffffffffu, r1[c], o);
+                r2[c] += __shfl_xor_sync(0xffffffffu, r2[c], o);
+            }
+        if (NT == 32) {
+            if (lane == 0)
+#pragma unroll
+                for (int c = 0; c < NC; c++) {
+                    if (MODE == MODE_GRAD) {
+                        qsum[c] += wkl * r1[c];
+                    } else {
+                        qsum[2 * c] += r1[c];
+                        qsum[2 * c + 1] += r2[c];
+                    }
+                }
+        } else {
+            // CTA: per-warp partials through shared memory, fixed-order sum
+            __syncthreads();
+            double *red = wsm;
+            if ((lane & 31) == 0)
+#pragma unroll
+                for (int c = 0; c < NC; c++) {
+                    red[(lane >> 5) * 6 + 2 * c] = r1[c];
+                    red[(lane >> 5) * 6 + 2 * c + 1] = r2[c];
+                }
+            __syncthreads();
+            if (lane == 0)
+#pragma unroll
+                for (int c = 0; c < NC; c++) {
+                    double a = 0.0, b = 0.0;
+                    for (int w = 0; w < NT / 32; w++) {
+                        a += red[w * 6 + 2 * c];
+                        b += red[w * 6 + 2 * c + 1];
+                    }
+                    if (MODE == MODE_GRAD) {
+                        qsum[c] = wkl * a;
+                    } else {
+                        qsum[2 * c] = a;
+                        qsum[2 * c + 1] = b;
+                    }
+                }
+            __syncthreads();
+        }
+    }
+}
+
+// Dispatch on the accumulator capacity per thread, so the unrolled per-slot
+// loop carries no predicated-off iterations beyond the next multiple of 8.
+template <int D, int MODE>
+__device__ __forceinline__ void eri_quartet_hc_any(const int *__restrict__ atm, const int *__restrict__ bas,
+                                                   const double *__restrict__ env, const int *__restrict__ ao_loc,
+                                                   int ish, int jsh, int ksh, int lsh, const HcPlan &h,
+                                                   double *__restrict__ wsm, const S2klOut &so,
+                                                   double *__restrict__ qsum, int lane)
+{
+    const int nj = (h.nacc + 31) / 32;
+    if (nj <= 8)
+        eri_quartet_hc<D, MODE, 8, 32>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, h, wsm, so, qsum, lane, kHcSmem);
+    else if (nj <= 16)
+        eri_quartet_hc<D, MODE, 16, 32>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, h, wsm, so, qsum, lane, kHcSmem);
+    else if (nj <= 24)
+        eri_quartet_hc<D, MODE, 24, 32>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, h, wsm, so, qsum, lane, kHcSmem);
+    else if (nj <= 32)
+        eri_quartet_hc<D, MODE, 32, 32>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, h, wsm, so, qsum, lane, kHcSmem);
+    else
+        eri_quartet_hc<D, MODE, kHcMaxJ, 32>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, h, wsm, so, qsum, lane,
+                                             kHcSmem);
+}
+
+// Heavy quartets (CTA of 256 threads): up to 16 accumulators per thread.
+static constexpr int kHcCtaMaxJ = 16;
+
+template <int D, int MODE>
+__device__ __forceinline__ void eri_quartet_hc_cta(const int *__restrict__ atm, const int *__restrict__ bas,
+                                                   const double *__restrict__ env, const int *__restrict__ ao_loc,
+                                                   int ish, int jsh, int ksh, int lsh, const HcPlan &h,
+                                                   double *__restrict__ sm, int cap, const S2klOut &so,
+                                                   double *__restrict__ qsum)
+{
+    if (h.nacc <= 256 * 8)
+        eri_quartet_hc<D, MODE, 8, 256>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, h, sm, so, qsum, threadIdx.x, cap);
+    else
+        eri_quartet_hc<D, MODE, kHcCtaMaxJ, 256>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, h, sm, so, qsum,
+                                                 threadIdx.x, cap);
+}
+
 // Quartets whose Cartesian block has more functions than this go to the
 // CTA-cooperative kernel; smaller ones are one warp each.
 static constexpr int kHeavyNf = 1000;
@@ -666,7 +1156,7 @@ __device__ __forceinline__ void decode_pair(long long p, int &k, int &l)
 
 // s2kl block of shells [ish0, ish1) x all j x all k >= l (decontracted shells).
 template <int D, bool LOW>
-__global__ void __launch_bounds__(kWarps * 32, LOW ? (D ? 2 : 3) : 2) eri_s2kl_kernel(
+__global__ void __launch_bounds__(kWarps * 32, 2) eri_s2kl_kernel(
     const int *__restrict__ atm, const int *__restrict__ bas, const double *__restrict__ env,
     const int *__restrict__ ao_loc, int ish0, int ish1, int nbas, int nao, double *__restrict__ out,
     int smem_warp)
@@ -688,6 +1178,14 @@ __global__ void __launch_bounds__(kWarps * 32, LOW ? (D ? 2 : 3) : 2) eri_s2kl_k
         decode_pair(q - ij * npairs, ksh, lsh);
         const int ish = ish0 + (int)(ij / nbas), jsh = (int)(ij % nbas);
         if (quartet_nf(bas, ish, jsh, ksh, lsh) > kHeavyNf) continue;
+        if (LOW) {
+            HcPlan h;
+            if (hc_plan(D, bas[ish * CB_BAS_SLOTS + CB_ANG_OF], bas[jsh * CB_BAS_SLOTS + CB_ANG_OF],
+                        bas[ksh * CB_BAS_SLOTS + CB_ANG_OF], bas[lsh * CB_BAS_SLOTS + CB_ANG_OF], h)) {
+                eri_quartet_hc_any<D, MODE_S2KL>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, h, wsm, so, nullptr, lane);
+                continue;
+            }
+        }
         eri_quartet<D, MODE_S2KL, LOW>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, wsm, smem_warp, so, nullptr, lane);
     }
 }
@@ -695,7 +1193,7 @@ __global__ void __launch_bounds__(kWarps * 32, LOW ? (D ? 2 : 3) : 2) eri_s2kl_k
 // Explicit quartet list (int4 shells): MODE_QSUM writes two checksums per
 // component per quartet, MODE_GRAD one gamma contraction per component.
 template <int D, bool LOW, int MODE = MODE_QSUM>
-__global__ void __launch_bounds__(kWarps * 32, LOW ? (D ? 2 : 3) : 2) eri_qsum_kernel(
+__global__ void __launch_bounds__(kWarps * 32, 2) eri_qsum_kernel(
     const int *__restrict__ atm, const int *__restrict__ bas, const double *__restrict__ env,
     const int4 *__restrict__ quartets, long long nq, double *__restrict__ qsum, int smem_warp,
     const int *__restrict__ ao_loc = nullptr, const double *__restrict__ gamma = nullptr, int nao = 0)
@@ -708,12 +1206,24 @@ __global__ void __launch_bounds__(kWarps * 32, LOW ? (D ? 2 : 3) : 2) eri_qsum_k
     so.nao = nao;
     constexpr int NC = D ? 3 : 1;
     constexpr int NOUT = MODE == MODE_QSUM ? 2 * NC : NC;
-    for (long long q = (long long)blockIdx.x * kWarps + warp; q < nq; q += (long long)gridDim.x * kWarps) {
+    // lists are L-class ordered, cheap classes first: walk them from the end
+    // so the expensive quartets start first and cheap ones fill the tail.  A
+    // block takes one contiguous chunk, so its warps run the same class (and
+    // code path) at the same time.
+    const long long per = (nq + gridDim.x - 1) / gridDim.x;
+    const long long t0 = (long long)blockIdx.x * per, t1 = t0 + per < nq ? t0 + per : nq;
+    for (long long t = t0 + warp; t < t1; t += kWarps) {
+        const long long q = nq - 1 - t;
         const int4 s = quartets[q];
         if (quartet_nf(bas, s.x, s.y, s.z, s.w) > kHeavyNf) continue;
         double acc[NOUT];
         for (int c = 0; c < NOUT; c++) acc[c] = 0.0;
-        eri_quartet<D, MODE, LOW>(atm, bas, env, ao_loc, s.x, s.y, s.z, s.w, wsm, smem_warp, so, acc, lane);
+        HcPlan h;
+        if (LOW && hc_plan(D, bas[s.x * CB_BAS_SLOTS + CB_ANG_OF], bas[s.y * CB_BAS_SLOTS + CB_ANG_OF],
+                           bas[s.z * CB_BAS_SLOTS + CB_ANG_OF], bas[s.w * CB_BAS_SLOTS + CB_ANG_OF], h))
+            eri_quartet_hc_any<D, MODE>(atm, bas, env, ao_loc, s.x, s.y, s.z, s.w, h, wsm, so, acc, lane);
+        else
+            eri_quartet<D, MODE, LOW>(atm, bas, env, ao_loc, s.x, s.y, s.z, s.w, wsm, smem_warp, so, acc, lane);
         if (lane == 0)
             for (int c = 0; c < NOUT; c++) qsum[q * NOUT + c] = acc[c];
     }
@@ -735,6 +1245,14 @@ __global__ void __launch_bounds__(kHeavyThreads, 1) eri_s2kl_heavy_kernel(
     so.i_base = ao_loc[ish0];
     for (long long q = blockIdx.x; q < nq; q += gridDim.x) {
         const int4 s = quartets[q];
+        HcPlan h;
+        if (LOW && hc_plan(D, bas[s.x * CB_BAS_SLOTS + CB_ANG_OF], bas[s.y * CB_BAS_SLOTS + CB_ANG_OF],
+                           bas[s.z * CB_BAS_SLOTS + CB_ANG_OF], bas[s.w * CB_BAS_SLOTS + CB_ANG_OF], h,
+                           256 * kHcCtaMaxJ, smem_doubles, true)) {
+            eri_quartet_hc_cta<D, MODE_S2KL>(atm, bas, env, ao_loc, s.x, s.y, s.z, s.w, h, smem, smem_doubles, so,
+                                             nullptr);
+            continue;
+        }
         eri_quartet_cta<D, MODE_S2KL, LOW>(atm, bas, env, ao_loc, s.x, s.y, s.z, s.w, smem, smem_doubles, so, nullptr);
     }
 }
@@ -755,6 +1273,14 @@ __global__ void __launch_bounds__(kHeavyThreads, 1) eri_qsum_heavy_kernel(
     for (long long q = blockIdx.x; q < nq; q += gridDim.x) {
         const int4 s = quartets[q];
         if (quartet_nf(bas, s.x, s.y, s.z, s.w) <= kHeavyNf) continue;
+        HcPlan h;
+        if (LOW && hc_plan(D, bas[s.x * CB_BAS_SLOTS + CB_ANG_OF], bas[s.y * CB_BAS_SLOTS + CB_ANG_OF],
+                           bas[s.z * CB_BAS_SLOTS + CB_ANG_OF], bas[s.w * CB_BAS_SLOTS + CB_ANG_OF], h,
+                           256 * kHcCtaMaxJ, smem_doubles, true)) {
+            eri_quartet_hc_cta<D, MODE>(atm, bas, env, ao_loc, s.x, s.y, s.z, s.w, h, smem, smem_doubles, so,
+                                        qsum + q * NOUT);
+            continue;
+        }
         eri_quartet_cta<D, MODE, LOW>(atm, bas, env, ao_loc, s.x, s.y, s.z, s.w, smem, smem_doubles, so,
                                       qsum + q * NOUT);
     }
@@ -836,6 +1362,7 @@ static int smem_per_warp(int lmax, int deriv)
 {
     const int gsz = (lmax + 1 + deriv) * (lmax + 1) * (lmax + 1) * (lmax + 1);
     int need = 3 * gsz + kParStride;
+    if (lmax <= 2 && need < kHcSmem) need = kHcSmem;     // contracted-HRR path
     return need < 2048 ? 2048 : need;
 }
 
