@@ -20,8 +20,15 @@ Other workloads (``--workload``):
           H at (0, +-0.757, 0.587) A): RHF + CCSD + Lambda + gradient per step,
           FP64 mode and the split-precision mode; grads/s and max|dg| between
           them; the numpy restatement of the same chain timed on the host.
+  autograd  CCSDEnergy (torch.autograd.Function) forward + backward for
+          ethanol/cc-pVDZ (seeded N(0, 0.02 A) displacements), FP64 and split
+          precision; backward checked against central finite differences
+          (1e-3 bohr, all 27 coordinates, FP64 energies).
+  clusters  gradients of seeded water clusters (H2O)n, n uniform in 1..6,
+          cc-pVDZ, one after another through the same chain, FP64 and split
+          precision; molecules/s and per-molecule max|dg| vs FP64.
 
-  python bench.py [--workload eri|lambda|gemm|grad] [--gpus N] [--steps K] [--warmup W]
+  python bench.py [--workload eri|lambda|gemm|grad|autograd|clusters] [--gpus N] [--steps K] [--warmup W]
                   [--impl ours|reference]
 
 Multi-GPU (torchrun): every rank runs its own copy of the workload (weak
@@ -46,7 +53,9 @@ NSHELL = 4096
 
 def parse():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", choices=["eri", "lambda", "gemm", "grad"], default="eri")
+    ap.add_argument("--workload", choices=["eri", "lambda", "gemm", "grad", "autograd", "clusters"], default="eri")
+    ap.add_argument("--molecules", type=int, default=16, help="clusters workload: molecules per step (64 = full set)")
+    ap.add_argument("--no-fd", action="store_true", help="autograd workload: skip the finite-difference check")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=None)
@@ -60,7 +69,8 @@ def parse():
     ap.add_argument("--quartets", type=int, default=1 << 18, help="sampled quartets per rank per step")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU-baseline sample budget")
     args = ap.parse_args()
-    dflt = {"eri": (10, 3), "lambda": (3, 3), "gemm": (10, 3), "grad": (5, 3)}[args.workload]
+    dflt = {"eri": (10, 3), "lambda": (3, 3), "gemm": (10, 3), "grad": (5, 3), "autograd": (3, 3),
+            "clusters": (1, 1)}[args.workload]     # clusters: one warm-up pass fills the basis caches
     args.steps = dflt[0] if args.steps is None else args.steps
     args.warmup = dflt[1] if args.warmup is None else args.warmup
     return args
@@ -425,6 +435,132 @@ def run_grad(args, ws, rank, local):
         print(json.dumps(line), flush=True)
 
 
+
+def _ccsd_energy(mol, mode):
+    from ccsd_gpu_b200.ccsd import CCSD
+    from ccsd_gpu_b200.scf import RHF
+    cc = CCSD(RHF(mol).run(), precision=mode)
+    cc.kernel()
+    return cc.e_tot
+
+
+def run_autograd(args, ws, rank, local):
+    """CCSDEnergy forward + backward for ethanol/cc-pVDZ; central-FD check."""
+    from ccsd_gpu_b200 import workloads
+    from ccsd_gpu_b200.gpu_ccsd_grad import CCSDEnergy
+    from ccsd_gpu_b200.gto import M
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    barrier = (lambda: (torch.distributed.barrier(), torch.cuda.synchronize(dev))) if ws > 1 else \
+        (lambda: torch.cuda.synchronize(dev))
+    sym, xyz = workloads.ethanol_atoms(seed=0)
+    mol = M(atom=workloads.atom_string(sym, xyz), basis="cc-pvdz")
+    x0 = torch.tensor(mol.atom_coords(), dtype=torch.float64)
+    grads = {}
+
+    def step(mode):
+        def run():
+            x = x0.to(dev).requires_grad_(True)
+            e = CCSDEnergy.apply(x, mol, mode)
+            e.backward()
+            grads[mode] = x.grad.detach().cpu().numpy()
+        return run
+
+    res = {}
+    for mode in ("fp64", args.mode):
+        fn = step(mode)
+        for _ in range(args.warmup):
+            fn()
+        with ClockSampler(dev) as clk:
+            ks, _ = _events_timed(fn, args.steps, barrier)
+        res[mode] = {"s_per_grad": _maxr(float(ks.mean()), ws, dev) * 1e-3, "clocks": clk.summary()}
+    fd_err = None
+    if not args.no_fd and rank == 0:
+        h = 1e-3
+        fd = np.zeros_like(grads["fp64"])
+        for a in range(mol.natm):
+            for c in range(3):
+                ep = []
+                for sgn in (1, -1):
+                    xs = x0.numpy().copy()
+                    xs[a, c] += sgn * h
+                    ep.append(_ccsd_energy(mol.copy().set_geom_(xs), "fp64"))
+                fd[a, c] = (ep[0] - ep[1]) / (2 * h)
+        fd_err = {"max_abs_fd_minus_fp64_backward": float(np.abs(fd - grads["fp64"]).max()),
+                  "max_abs_fd_minus_mixed_backward": float(np.abs(fd - grads[args.mode]).max()),
+                  "step_bohr": h, "coordinates": int(fd.size)}
+    mx = res[args.mode]
+    line = {"metric": "CCSDEnergy forward+backward per s, ethanol/cc-pVDZ, %s vs FP64" % args.mode,
+            "value": ws / mx["s_per_grad"], "unit": "grads/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": mx["s_per_grad"] * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": args.mode, "data": "synthetic",
+            "config": {"workload": "ethanol_ccpvdz_autograd", "nao": mol.nao_nr(), "nocc": mol.nelectron // 2,
+                       "geometry": "standard internal coordinates + N(0, 0.02 A) displacements, seed 0",
+                       "parallelism": "dp%d" % ws if ws > 1 else "single"},
+            "fp64_grads_per_s": ws / res["fp64"]["s_per_grad"], "mixed_grads_per_s": ws / mx["s_per_grad"],
+            "speedup_vs_fp64": res["fp64"]["s_per_grad"] / mx["s_per_grad"],
+            "max_abs_dg_vs_fp64": float(np.abs(grads[args.mode] - grads["fp64"]).max()),
+            "finite_difference": fd_err, "roofline": None, "clocks": mx["clocks"], "cpu_baseline": None,
+            "e2e": None}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_clusters(args, ws, rank, local):
+    """Gradients of seeded water clusters, FP64 and split precision."""
+    from ccsd_gpu_b200 import workloads
+    from ccsd_gpu_b200.ccsd import CCSD
+    from ccsd_gpu_b200.gto import M
+    from ccsd_gpu_b200.scf import RHF
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    barrier = (lambda: (torch.distributed.barrier(), torch.cuda.synchronize(dev))) if ws > 1 else \
+        (lambda: torch.cuda.synchronize(dev))
+    allc = workloads.water_clusters(64, seed=0)
+    # rank r takes every ws-th cluster of the first args.molecules * ws (weak scaling)
+    mine = [allc[i % 64] for i in range(rank, args.molecules * ws, ws)]
+    mols = [M(atom=workloads.atom_string(s, x), basis="cc-pvdz") for s, x in mine]
+    grads = {}
+
+    def step(mode):
+        def run():
+            out = []
+            for mol in mols:
+                cc = CCSD(RHF(mol).run(), precision=mode)
+                cc.kernel()
+                cc.conv_tol_normt = 1e-9
+                out.append(cc.nuc_grad_method().kernel())
+            grads[mode] = out
+        return run
+
+    res = {}
+    for mode in ("fp64", args.mode):
+        fn = step(mode)
+        for _ in range(args.warmup):
+            fn()
+        with ClockSampler(dev) as clk:
+            ks, _ = _events_timed(fn, args.steps, barrier)
+        res[mode] = {"s_per_batch": _maxr(float(ks.mean()), ws, dev) * 1e-3, "clocks": clk.summary()}
+    dg = [float(np.abs(a - b).max()) for a, b in zip(grads[args.mode], grads["fp64"])]
+    nper = [m.natm // 3 for m in mols]
+    mx = res[args.mode]
+    line = {"metric": "CCSD gradients of (H2O)n clusters, n in 1..6, cc-pVDZ: molecules/s, %s vs FP64" % args.mode,
+            "value": len(mols) * ws / mx["s_per_batch"], "unit": "molecules/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": mx["s_per_batch"] * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": args.mode,
+            "data": "synthetic",
+            "config": {"workload": "water_clusters_ccpvdz", "molecules_per_rank": len(mols),
+                       "waters_per_molecule": nper, "cluster_set": "64 seeded clusters (seed 0), first %d"
+                       % (len(mols) * ws), "parallelism": "dp%d" % ws if ws > 1 else "single"},
+            "fp64_molecules_per_s": len(mols) * ws / res["fp64"]["s_per_batch"],
+            "mixed_molecules_per_s": len(mols) * ws / mx["s_per_batch"],
+            "speedup_vs_fp64": res["fp64"]["s_per_batch"] / mx["s_per_batch"],
+            "per_molecule_max_abs_dg_vs_fp64": dg, "max_abs_dg_vs_fp64": max(dg),
+            "roofline": None, "clocks": mx["clocks"], "cpu_baseline": None, "e2e": None}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     ws, rank, local = dist_setup()
@@ -434,7 +570,8 @@ def main():
             torch.distributed.destroy_process_group()
         return
     if args.workload != "eri":
-        {"gemm": run_gemm, "lambda": run_lambda, "grad": run_grad}[args.workload](args, ws, rank, local)
+        {"gemm": run_gemm, "lambda": run_lambda, "grad": run_grad, "autograd": run_autograd,
+         "clusters": run_clusters}[args.workload](args, ws, rank, local)
         if ws > 1:
             torch.distributed.destroy_process_group()
         return

@@ -207,3 +207,101 @@ def lambda_bench_state(nocc=24, nvir=216, seed=0, device="cuda", eri_sigma=0.05,
     d2 = (eia[:, None, :, None] + eia[None, :, None, :]).abs()
     t2 = (x + x.permute(1, 0, 3, 2)) * (1e-2 / np.sqrt(2.0)) / (1 + d2)
     return eris, t1, t2
+
+
+# ---- molecules of the gradient workloads ---------------------------------------------
+def _zmat_to_xyz(rows):
+    """Cartesian coordinates from (symbol, (i, r), (j, angle_deg), (k, dihedral_deg)) rows."""
+    xyz = []
+    for n, row in enumerate(rows):
+        if n == 0:
+            xyz.append(np.zeros(3))
+            continue
+        (i, r) = row[1]
+        if n == 1:
+            xyz.append(xyz[i] + np.array([r, 0.0, 0.0]))
+            continue
+        (j, ang) = row[2]
+        a = np.radians(ang)
+        if n == 2:
+            u = (xyz[j] - xyz[i]) / np.linalg.norm(xyz[j] - xyz[i])
+            v = np.array([-u[1], u[0], 0.0]) if abs(u[2]) < 0.9 else np.array([0.0, -u[2], u[1]])
+            v /= np.linalg.norm(v)
+            xyz.append(xyz[i] + r * (np.cos(a) * u + np.sin(a) * v))
+            continue
+        (k, dih) = row[3]
+        d = np.radians(dih)
+        b = xyz[i] - xyz[j]
+        c = xyz[k] - xyz[j]
+        nrm = np.cross(b, c)
+        nrm /= np.linalg.norm(nrm)
+        m = np.cross(nrm, b / np.linalg.norm(b))
+        local = np.array([-r * np.cos(a), r * np.sin(a) * np.cos(d), r * np.sin(a) * np.sin(d)])
+        bu = b / np.linalg.norm(b)
+        xyz.append(xyz[i] + local[0] * bu + local[1] * m + local[2] * nrm)
+    return np.array(xyz)
+
+
+ETHANOL_ZMAT = [
+    ("C",), ("C", (0, 1.512)), ("O", (1, 1.425), (0, 108.0)),
+    ("H", (2, 0.962), (1, 108.5), (0, 180.0)),
+    ("H", (1, 1.094), (2, 110.0), (3, 60.0)), ("H", (1, 1.094), (2, 110.0), (3, -60.0)),
+    ("H", (0, 1.091), (1, 110.8), (2, 180.0)), ("H", (0, 1.091), (1, 110.8), (2, 60.0)),
+    ("H", (0, 1.091), (1, 110.8), (2, -60.0)),
+]
+
+
+def ethanol_atoms(seed=0, sigma=0.02):
+    """Ethanol (anti conformer) from standard bond lengths and angles
+    (C-C 1.512, C-O 1.425, O-H 0.962, C-H 1.09 A; tetrahedral angles,
+    staggered), displaced by seeded N(0, sigma A) noise: (symbols, xyz in A)."""
+    xyz = _zmat_to_xyz(ETHANOL_ZMAT)
+    xyz = xyz + np.random.default_rng(seed).normal(0.0, sigma, xyz.shape)
+    return [r[0] for r in ETHANOL_ZMAT], xyz
+
+
+_WATER = np.array([[0.0, 0.0, 0.0], [0.0, 0.757, 0.587], [0.0, -0.757, 0.587]])   # O, H, H (A)
+
+
+def _rotation(rng):
+    q = rng.normal(size=4)
+    q /= np.linalg.norm(q)
+    a, b, c, d = q
+    return np.array([[a * a + b * b - c * c - d * d, 2 * (b * c - a * d), 2 * (b * d + a * c)],
+                     [2 * (b * c + a * d), a * a - b * b + c * c - d * d, 2 * (c * d - a * b)],
+                     [2 * (b * d - a * c), 2 * (c * d + a * b), a * a - b * b - c * c + d * d]])
+
+
+def water_cluster_atoms(n, rng):
+    """(H2O)n: each new oxygen 2.8 +- 0.2 A (uniform) from a randomly chosen
+    earlier one and at least 2.5 A from all others, randomly oriented
+    monomers with H atoms kept 1.5 A from other molecules' atoms."""
+    mols = []
+    for m in range(n):
+        for _ in range(1000):
+            R = _rotation(rng)
+            if m == 0:
+                centre = np.zeros(3)
+            else:
+                d = rng.normal(size=3)
+                d /= np.linalg.norm(d)
+                centre = mols[rng.integers(m)][0] + rng.uniform(2.6, 3.0) * d
+            w = centre + _WATER @ R.T
+            if all(np.linalg.norm(w[0] - o[0]) >= 2.5 for o in mols) and \
+               all(np.linalg.norm(a - b) >= 1.5 for o in mols for a in w for b in o):
+                mols.append(w)
+                break
+        else:
+            raise RuntimeError("could not place water %d" % m)
+    xyz = np.concatenate(mols, 0)
+    return ["O", "H", "H"] * n, xyz
+
+
+def water_clusters(count=64, seed=0, nmax=6):
+    """`count` seeded clusters (H2O)n, n uniform in 1..nmax: list of (symbols, xyz A)."""
+    rng = np.random.default_rng(seed)
+    return [water_cluster_atoms(int(rng.integers(1, nmax + 1)), rng) for _ in range(count)]
+
+
+def atom_string(symbols, xyz):
+    return "; ".join("%s %.10f %.10f %.10f" % (s, *p) for s, p in zip(symbols, xyz))
