@@ -16,6 +16,7 @@ import torch
 
 from . import _native
 from .contract import check_status, contract
+from .graphs import StepGraph
 from .gpu_ccsd_lambda import DIIS, DeviceEris, amplitude_norm_sq, solve_lambda_gpu
 
 
@@ -146,6 +147,11 @@ class CCSD:
         self.lambda_polish = True
         self.diis_space = 8
         self.level_shift = 0.0
+        # replay the T / Lambda update bodies as CUDA graphs.  Off by default:
+        # one capture per solve (eager + warm-up + capture) costs about as much
+        # as it saves over the 12-20 iterations of one gradient (measured on
+        # H2O and (H2O)6, cc-pVDZ)
+        self.use_graphs = False
         self.verbose = 0
         self.t1 = self.t2 = self.l1 = self.l2 = None
         self.converged = self.converged_lambda = False
@@ -177,8 +183,9 @@ class CCSD:
         mode = self.precision
         tol_n = self.conv_tol_normt if mode == "fp64" else max(self.conv_tol_normt, 1e-6)
         self._t_history = []
+        step = self._step(eris, mode)
         for it in range(self.max_cycle):
-            t1n, t2n = update_amps_gpu(t1, t2, eris, mode, self.level_shift)
+            t1n, t2n = step(t1, t2)
             normt = float(torch.sqrt(amplitude_norm_sq(t1n - t1, t2n - t2)))
             self._t_history.append((mode, normt))
             x = adiis.update(torch.cat([t1n.reshape(-1), t2n.reshape(-1)]),
@@ -188,6 +195,7 @@ class CCSD:
             if normt < tol_n and abs(e - e_old) < self.conv_tol:
                 if mode != "fp64" and self.t_polish and self.conv_tol_normt < tol_n:
                     mode, tol_n = "fp64", self.conv_tol_normt
+                    step = self._step(eris, mode)
                     adiis = DIIS(self.diis_space)
                     e_old = e
                     continue
@@ -199,6 +207,10 @@ class CCSD:
         self._t1g, self._t2g = t1, t2
         self.t1, self.t2 = t1.cpu().numpy(), t2.cpu().numpy()
         return self.e_corr, self.t1, self.t2
+
+    def _step(self, eris, mode):
+        ls = self.level_shift
+        return StepGraph(lambda a, b: update_amps_gpu(a, b, eris, mode, ls), enabled=self.use_graphs)
 
     @property
     def e_tot(self):

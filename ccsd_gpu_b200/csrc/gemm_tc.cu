@@ -442,9 +442,17 @@ static int launch_tc(const CUtensorMap &ma, const CUtensorMap &mal, const CUtens
                      cudaStream_t st)
 {
     const size_t smem = TC_STAGES * TC_STAGE_BYTES + 1024;
-    if (cudaFuncSetAttribute(tc_split_gemm_kernel<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-        cudaSuccess)
-        return check_launch("cudaFuncSetAttribute(tc_split_gemm_kernel)");
+    // the attribute is set once per device: launches may be captured into
+    // CUDA graphs, and nothing but the launch itself should run per call
+    static bool attr_set[KIND_BF16 + 1][64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return check_launch("cudaGetDevice");
+    if (!attr_set[KIND][dev]) {
+        if (cudaFuncSetAttribute(tc_split_gemm_kernel<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem) != cudaSuccess)
+            return check_launch("cudaFuncSetAttribute(tc_split_gemm_kernel)");
+        attr_set[KIND][dev] = true;
+    }
     const int mt = (m_pad + TC_BM - 1) / TC_BM, nt = (n_pad + TC_BN - 1) / TC_BN;
     const int per = (kblocks + ksplit - 1) / ksplit;
     const int nsplit = (kblocks + per - 1) / per;           // every split non-empty

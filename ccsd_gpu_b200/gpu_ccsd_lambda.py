@@ -25,6 +25,7 @@ import torch
 
 from . import _native
 from .contract import check_status, contract, mark_constant
+from .graphs import StepGraph
 
 DEFAULT_MODE = "tf32x3"
 
@@ -296,8 +297,14 @@ def kernel_gpu(mycc, eris=None, t1=None, t2=None, l1=None, l2=None, max_cycle=No
     nov = l1g.numel()
     conv = False
     history = []
+    graphs = getattr(mycc, "use_graphs", False)
+
+    def make_step(im, md):
+        return StepGraph(lambda a, b: update_lambda_gpu(mycc, t1g, t2g, a, b, eris, im, mode=md), enabled=graphs)
+
+    step = make_step(imds, cur_mode)
     for istep in range(max_cycle):
-        l1n, l2n = update_lambda_gpu(mycc, t1g, t2g, l1g, l2g, eris, imds, mode=cur_mode)
+        l1n, l2n = step(l1g, l2g)
         normt = float(torch.sqrt(amplitude_norm_sq(l1n - l1g, l2n - l2g)))
         history.append((cur_mode, normt))
         if adiis is not None:
@@ -310,6 +317,7 @@ def kernel_gpu(mycc, eris=None, t1=None, t2=None, l1=None, l2=None, max_cycle=No
             if cur_mode != "fp64" and polish and tol < cur_tol:
                 cur_mode, cur_tol = "fp64", tol
                 imds = make_intermediates_gpu(mycc, t1g, t2g, eris, "fp64")
+                step = make_step(imds, cur_mode)
                 adiis = DIIS(space) if use_diis else None
                 continue
             conv = normt < tol or (cur_mode != "fp64" and not polish)

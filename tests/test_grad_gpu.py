@@ -103,3 +103,22 @@ def test_autograd_energy_backward_and_finite_difference():
             y[a, c] += s * h
             xs.append(float(CCSDEnergy.apply(y, mol, "fp64")))
         assert abs((xs[0] - xs[1]) / (2 * h) - float(x.grad[a, c])) < 5e-7
+
+
+@pytest.mark.parametrize("mode", ["fp64", "tf32x3"])
+def test_cuda_graph_replay_matches_eager(mode):
+    """The T and Lambda updates replayed as CUDA graphs give the eager results."""
+    from ccsd_gpu_b200.ccsd import CCSD
+    from ccsd_gpu_b200.gto import M
+    from ccsd_gpu_b200.scf import RHF
+    mf = RHF(M(atom=H2O, basis="cc-pvdz")).run()
+    out = {}
+    for graphs in (False, True):
+        cc = CCSD(mf, precision=mode)
+        cc.use_graphs = graphs
+        cc.kernel()
+        cc.conv_tol_normt = 1e-9
+        cc.solve_lambda()
+        out[graphs] = (cc.e_tot, cc.nuc_grad_method().kernel())
+    assert abs(out[True][0] - out[False][0]) < 1e-10
+    assert np.abs(out[True][1] - out[False][1]).max() < 1e-9
