@@ -15,7 +15,7 @@ import numpy as np
 import torch
 
 from . import _native
-from .contract import check_status, contract
+from .contract import check_status, contract, effective_mode
 from .graphs import StepGraph
 from .gpu_ccsd_lambda import DIIS, DeviceEris, amplitude_norm_sq, solve_lambda_gpu
 
@@ -180,7 +180,7 @@ class CCSD:
         self.converged = False
         # split precision down to its ~1e-6 noise floor, then FP64 iterations
         # (mixed-precision iterative refinement; ``t_polish = False`` skips them)
-        mode = self.precision
+        mode = effective_mode(self.precision, nocc, t1.shape[1])
         tol_n = self.conv_tol_normt if mode == "fp64" else max(self.conv_tol_normt, 1e-6)
         self._t_history = []
         step = self._step(eris, mode)

@@ -196,6 +196,20 @@ def _pack_new(terms, sub, rows_idx, k_idx, shape_map, kind, rows_pad, k_pad, dev
 LOW_INTENSITY_K = 32
 LOW_INTENSITY_FLOP_PER_BYTE = 12.0
 LOW_INTENSITY_MAX_K = 1024
+# below this many flops a contraction is launch-bound: one cuBLAS call beats
+# two packs and a tensor-core launch, and FP64 is exact
+SMALL_FLOPS = 5e7
+
+
+def effective_mode(mode, nocc, nvir):
+    """The mode an iterative solver should run in: split precision gains
+    nothing when even its largest contraction (the o^2 v^4 ladder) is below
+    SMALL_FLOPS, since every contraction then takes the FP64 route anyway; the
+    solver runs in FP64 directly and skips the split-precision phase and the
+    FP64 polish after it."""
+    if mode != "fp64" and 2.0 * nocc * nocc * float(nvir) ** 4 < SMALL_FLOPS:
+        return "fp64"
+    return mode
 
 
 def _combine(terms):
@@ -264,8 +278,8 @@ def contract(spec, a, b, out=None, alpha=1.0, beta=0.0, mode="tf32x3", stream=No
     K = int(np.prod([shape_map[i] for i in k_idx])) if k_idx else 1
     if M == 0 or N == 0:
         return out
-    if K <= LOW_INTENSITY_K or (K <= LOW_INTENSITY_MAX_K and 2.0 * M * N * K <
-                                LOW_INTENSITY_FLOP_PER_BYTE * 8.0 * (M * K + N * K + M * N)):
+    if K <= LOW_INTENSITY_K or 2.0 * M * N * K < SMALL_FLOPS or (
+            K <= LOW_INTENSITY_MAX_K and 2.0 * M * N * K < LOW_INTENSITY_FLOP_PER_BYTE * 8.0 * (M * K + N * K + M * N)):
         # memory-bound shape: FP64 through cuBLAS moves fewer bytes than the
         # split/pack/tensor-core route and is exact to FP64
         return _fp64_contract(spec, ta, tb, shape_map, out, alpha, beta)

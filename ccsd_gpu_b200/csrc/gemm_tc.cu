@@ -87,15 +87,16 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
     return ok != 0;
 }
 
-// bounded wait: false (and `code` recorded in *status) after TC_WAIT_NS
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *status, int code)
+// bounded wait: false (and `code` recorded in *status) after `limit_ns`
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *status, int code,
+                                          unsigned long long limit_ns = TC_WAIT_NS)
 {
     const unsigned long long t0 = global_ns();
     for (unsigned it = 0;; it++) {
         if (mbar_try_wait(bar, parity)) return true;
         if ((it & 63) == 63) {
             if (*(volatile int *)status != 0) return false;       // another CTA already gave up
-            if (global_ns() - t0 > TC_WAIT_NS) break;
+            if (global_ns() - t0 > limit_ns) break;
         }
     }
     atomicCAS(status, 0, code);
@@ -346,6 +347,20 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_split_gemm_kernel(
     }
 }
 
+// ---- failure-path probe: the pipeline's bounded mbarrier wait on a barrier
+// that nothing arrives at.  The wait gives up after `limit_ns`, records
+// `code` in *status and the kernel returns normally (no trap), so the host
+// sees the error and the context stays usable.
+__global__ void wait_probe_kernel(int *__restrict__ status, unsigned long long limit_ns, int code)
+{
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        mbar_wait(&bar, 0, status, code, limit_ns);     // phase 0 never completes
+    }
+}
+
 // ---- split-K reduction: out = alpha * sum_s partial[s] + beta * out (fixed order) ----
 __global__ void splitk_reduce_kernel(const double *__restrict__ partial, int ksplit, int M, int N,
                                      double *__restrict__ out, const long long *__restrict__ off_m,
@@ -472,6 +487,16 @@ static int launch_tc(const CUtensorMap &ma, const CUtensorMap &mal, const CUtens
 using namespace cb;
 
 extern "C" {
+
+int ccsd_b200_wait_probe(int *status, long long limit_ns, int code, void *stream)
+{
+    if (!status || limit_ns <= 0 || limit_ns > 10000000000ll || code == 0) {
+        set_error("ccsd_b200_wait_probe: invalid argument");
+        return CCSD_B200_ERR_ARG;
+    }
+    wait_probe_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(status, (unsigned long long)limit_ns, code);
+    return check_launch("wait_probe_kernel");
+}
 
 int ccsd_b200_split_pack(int kind, const double *src1, const long long *o1r, const long long *o1k, double c1,
                          const double *src2, const long long *o2r, const long long *o2k, double c2, int rows, int K,

@@ -24,7 +24,7 @@ import numpy as np
 import torch
 
 from . import _native
-from .contract import check_status, contract, mark_constant
+from .contract import check_status, contract, effective_mode, mark_constant
 from .graphs import StepGraph
 
 DEFAULT_MODE = "tf32x3"
@@ -285,6 +285,7 @@ def kernel_gpu(mycc, eris=None, t1=None, t2=None, l1=None, l2=None, max_cycle=No
     mode = _mode_of(mycc, mode)
     polish = getattr(mycc, "lambda_polish", True) if polish is None else polish
     t1g, t2g, l1g, l2g = _t(t1), _t(t2), _t(l1), _t(l2)
+    mode = effective_mode(mode, *t1g.shape)
     if t1g.data_ptr() == l1g.data_ptr() or t2g.data_ptr() == l2g.data_ptr():
         l1g, l2g = l1g.clone(), l2g.clone()
     mark_constant(t1g, t2g)

@@ -141,6 +141,16 @@ int ccsd_b200_eri_ip1_contract(const int32_t *atm, const int32_t *bas, const dou
                                const long long *seg, int nseg, int lmax, double *qwork, double *out, void *stream);
 
 /*
+ * Failure-path probe (no counterpart in the reference): one thread waits,
+ * with the same bounded mbarrier wait the tensor-core GEMM pipeline uses, on
+ * a barrier that nothing arrives at.  After limit_ns (<= 10 s) of global
+ * timer the wait gives up, `code` is stored in *status (if it was 0) and the
+ * kernel returns normally, so the host reads the error and the context stays
+ * usable.  Used by the tests of the timeout path.
+ */
+int ccsd_b200_wait_probe(int *status, long long limit_ns, int code, void *stream);
+
+/*
  * Split-precision tensor-core contraction, step 1: gather + split.
  *   v[r][k] = c1 * src1[o1r[r] + o1k[k]] + c2 * src2[o2r[r] + o2k[k]]   (src2 may be NULL)
  * for r < rows, k < K (zero elsewhere), written as hi + lo parts, K-major,

@@ -27,8 +27,10 @@ def test_plain_gemm(mode, tol):
         assert _rel(got, ref) < tol, (M, N, K, _rel(got, ref))
 
 
-def test_permuted_contraction_with_combined_operand_and_beta():
+def test_permuted_contraction_with_combined_operand_and_beta(monkeypatch):
+    import ccsd_gpu_b200.contract as C
     from ccsd_gpu_b200.contract import check_status, contract
+    monkeypatch.setattr(C, "SMALL_FLOPS", 0.0)      # keep this small case on the tensor cores
     g = torch.Generator(device="cuda").manual_seed(1)
     o, v = 6, 23
     ovvv = torch.randn(o, v, v, v, dtype=torch.float64, device="cuda", generator=g)
@@ -74,8 +76,8 @@ def test_tall_skinny_more_than_65535_row_tiles():
 def test_packed_operand_cache_follows_in_place_updates():
     from ccsd_gpu_b200.contract import _pack_cache, check_status, contract, mark_constant
     g = torch.Generator(device="cuda").manual_seed(4)
-    a = torch.randn(300, 200, dtype=torch.float64, device="cuda", generator=g)
-    b = torch.randn(100, 200, dtype=torch.float64, device="cuda", generator=g)
+    a = torch.randn(600, 800, dtype=torch.float64, device="cuda", generator=g)
+    b = torch.randn(400, 800, dtype=torch.float64, device="cuda", generator=g)
     mark_constant(b)
     n0 = len(_pack_cache)
     r1 = contract("mk,nk->mn", a, b)
@@ -128,6 +130,7 @@ def test_tensor_route_on_tiny_and_ragged_shapes(mode, tol, monkeypatch):
     import ccsd_gpu_b200.contract as C
     monkeypatch.setattr(C, "LOW_INTENSITY_K", 0)
     monkeypatch.setattr(C, "LOW_INTENSITY_FLOP_PER_BYTE", 0.0)
+    monkeypatch.setattr(C, "SMALL_FLOPS", 0.0)
     g = torch.Generator(device="cuda").manual_seed(7)
     for M, N, K in [(1, 7, 5), (128, 128, 40), (24, 5000, 24), (3, 1, 1)]:
         a = torch.randn(M, K, dtype=torch.float64, device="cuda", generator=g)

@@ -12,6 +12,14 @@ from tests.conftest import GOLDEN
 
 pytestmark = pytest.mark.gpu
 
+
+@pytest.fixture(autouse=True)
+def _tensor_cores_at_small_sizes(monkeypatch):
+    """These systems are small enough that every contraction would take the
+    launch-bound FP64 route; keep the split-precision modes on the tensor cores."""
+    import ccsd_gpu_b200.contract as Cn
+    monkeypatch.setattr(Cn, "SMALL_FLOPS", 0.0)
+
 H2O = "O 0 0 0; H 0 -0.757 0.587; H 0.05 0.757 0.587"
 
 
@@ -122,3 +130,18 @@ def test_cuda_graph_replay_matches_eager(mode):
         out[graphs] = (cc.e_tot, cc.nuc_grad_method().kernel())
     assert abs(out[True][0] - out[False][0]) < 1e-10
     assert np.abs(out[True][1] - out[False][1]).max() < 1e-9
+
+
+def test_nh3_gradient_matches_oracle_fp64_and_mixed():
+    """A second molecule (N with a d shell, three H) through the whole chain."""
+    from ccsd_gpu_b200.ccsd import CCSD
+    from ccsd_gpu_b200.gto import M
+    from ccsd_gpu_b200.scf import RHF
+    mol = M(atom="N 0 0 0.12; H 0 0.94 -0.28; H 0.81 -0.47 -0.28; H -0.80 -0.46 -0.30", basis="cc-pvdz")
+    _, g_ref = Q.ccsd_gradient(mol)
+    for mode, tol in (("fp64", 1e-7), ("tf32x3", 1e-6)):
+        cc = CCSD(RHF(mol).run(), precision=mode)
+        cc.kernel()
+        cc.conv_tol_normt = 1e-9
+        g = cc.nuc_grad_method().kernel()
+        assert np.abs(g - g_ref).max() < tol, (mode, np.abs(g - g_ref).max())

@@ -14,6 +14,14 @@ pytestmark = pytest.mark.gpu
 TOL = {"fp64": 1e-12, "tf32x3": 2e-6, "bf16x3": 2e-4}
 
 
+@pytest.fixture(autouse=True)
+def _tensor_cores_at_small_sizes(monkeypatch):
+    """These systems are small enough that every contraction would take the
+    launch-bound FP64 route; keep the split-precision modes on the tensor cores."""
+    import ccsd_gpu_b200.contract as Cn
+    monkeypatch.setattr(Cn, "SMALL_FLOPS", 0.0)
+
+
 @pytest.fixture(scope="module")
 def gold():
     d = dict(np.load(os.path.join(GOLDEN, "cc_small.npz")))
