@@ -396,16 +396,18 @@ def run_grad(args, ws, rank, local):
             grads[mode] = cc.nuc_grad_method().kernel()        # numpy (natm, 3): the D2H read
         return run
 
+    from ccsd_gpu_b200 import _native
     res = {}
     for mode in ("fp64", args.mode):
         fn = step(mode)
         for _ in range(args.warmup):
             fn()
         reset_stats()
+        n0 = sum(_native.CALLS.values())
         with ClockSampler(dev) as clk:
             ks, _ = _events_timed(fn, args.steps, barrier)
         res[mode] = {"s_per_grad": _maxr(float(ks.mean()), ws, dev) * 1e-3, "clocks": clk.summary(),
-                     "launches": STATS["launches"] // args.steps}
+                     "launches": (sum(_native.CALLS.values()) - n0) // args.steps}
     dg = float(np.abs(grads[args.mode] - grads["fp64"]).max())
     cpu = None
     if rank == 0 and ws == 1:

@@ -210,7 +210,23 @@ __device__ __forceinline__ void build_g_any(const double *__restrict__ p, int di
 #undef CB_G9
 #undef CB_G
 
-enum { MODE_S2KL = 0, MODE_QSUM = 1, MODE_GRAD = 2 };
+enum { MODE_S2KL = 0, MODE_QSUM = 1, MODE_GRAD = 2, MODE_FULL = 3 };
+
+// MODE_FULL (int2e over unique quartets): one integral into all eight index
+// orders of the dense [n]^4 tensor so.out (repeats for equal shells write the
+// same value twice).
+__device__ __forceinline__ void full_store8(double *__restrict__ g, long long n, long long i, long long j,
+                                            long long k, long long l, double v)
+{
+    g[((i * n + j) * n + k) * n + l] = v;
+    g[((j * n + i) * n + k) * n + l] = v;
+    g[((i * n + j) * n + l) * n + k] = v;
+    g[((j * n + i) * n + l) * n + k] = v;
+    g[((k * n + l) * n + i) * n + j] = v;
+    g[((l * n + k) * n + i) * n + j] = v;
+    g[((k * n + l) * n + j) * n + i] = v;
+    g[((l * n + k) * n + j) * n + i] = v;
+}
 
 struct S2klOut {
     double *out;
@@ -388,6 +404,20 @@ __device__ void eri_quartet(const int *__restrict__ atm, const int *__restrict__
                     const long long addr = ((long long)(i0 + fi) * so.nao + (j0 + fj)) * so.nao_pair + k * (k + 1) / 2 + l;
 #pragma unroll
                     for (int c = 0; c < NC; c++) so.out[c * so.comp_stride + addr] = acc[n][c];
+                }
+            }
+        } else if (MODE == MODE_FULL) {
+            const int i0 = ao_loc[ish], j0 = ao_loc[jsh], k0 = ao_loc[ksh], l0 = ao_loc[lsh];
+#pragma unroll
+            for (int n = 0; n < GW; n++) {
+                const int f = f0 + n * FW + flane;
+                if (f < nf && grp == 0) {
+                    int t = f;
+                    const int fl = t % nfl; t /= nfl;
+                    const int fk = t % nfk; t /= nfk;
+                    const int fj = t % nfj;
+                    const int fi = t / nfj;
+                    full_store8(so.out, so.nao, i0 + fi, j0 + fj, k0 + fk, l0 + fl, acc[n][0]);
                 }
             }
         } else if (MODE == MODE_GRAD) {
@@ -825,6 +855,8 @@ __device__ void eri_quartet_hc(const int *__restrict__ atm, const int *__restric
             const long long addr = ((long long)(i0 + oi) * so.nao + (j0 + oj)) * so.nao_pair + k * (k + 1) / 2 + l;
 #pragma unroll
             for (int c = 0; c < NC; c++) so.out[c * so.comp_stride + addr] = v[c];
+        } else if (MODE == MODE_FULL) {
+            full_store8(so.out, so.nao, ao_loc[ish] + oi, ao_loc[jsh] + oj, ao_loc[ksh] + fk, ao_loc[lsh] + fl, v[0]);
         } else if (MODE == MODE_GRAD) {
             const long long nao = so.nao;
             const int i0 = ao_loc[ish], j0 = ao_loc[jsh], k0 = ao_loc[ksh], l0 = ao_loc[lsh];
@@ -841,7 +873,7 @@ __device__ void eri_quartet_hc(const int *__restrict__ atm, const int *__restric
             }
         }
     }
-    if (MODE != MODE_S2KL) {
+    if (MODE == MODE_QSUM || MODE == MODE_GRAD) {
         const double wkl = MODE == MODE_GRAD && ksh != lsh ? 2.0 : 1.0;
 #pragma unroll
         for (int c = 0; c < NC; c++)
@@ -1097,6 +1129,20 @@ __device__ void eri_quartet_cta(const int *__restrict__ atm, const int *__restri
                            k * (k + 1) / 2 + l] = acc[n];
                 }
             }
+        } else if (MODE == MODE_FULL) {
+            const int i0 = ao_loc[ish], j0 = ao_loc[jsh], k0 = ao_loc[ksh], l0 = ao_loc[lsh];
+#pragma unroll
+            for (int n = 0; n < kHeavyAcc; n++) {
+                const int e = e0 + tid + n * kHeavyThreads;
+                if (e < ne) {
+                    int t = e / NC;
+                    const int fl = t % nfl; t /= nfl;
+                    const int fk = t % nfk; t /= nfk;
+                    const int fj = t % nfj;
+                    const int fi = t / nfj;
+                    full_store8(so.out, so.nao, i0 + fi, j0 + fj, k0 + fk, l0 + fl, acc[n]);
+                }
+            }
         } else if (MODE == MODE_GRAD) {
             const long long nao = so.nao;
             const int i0 = ao_loc[ish], j0 = ao_loc[jsh], k0 = ao_loc[ksh], l0 = ao_loc[lsh];
@@ -1126,7 +1172,7 @@ __device__ void eri_quartet_cta(const int *__restrict__ atm, const int *__restri
             }
         }
     }
-    if (MODE != MODE_S2KL) {
+    if (MODE == MODE_QSUM || MODE == MODE_GRAD) {
         constexpr int NOUT = MODE == MODE_QSUM ? 2 * NC : NC;
         const double wkl = MODE == MODE_GRAD && ksh != lsh ? 2.0 : 1.0;
         __shared__ double red[kHeavyThreads / 32][6];
@@ -1196,13 +1242,15 @@ template <int D, bool LOW, int MODE = MODE_QSUM>
 __global__ void __launch_bounds__(kWarps * 32, 2) eri_qsum_kernel(
     const int *__restrict__ atm, const int *__restrict__ bas, const double *__restrict__ env,
     const int4 *__restrict__ quartets, long long nq, double *__restrict__ qsum, int smem_warp,
-    const int *__restrict__ ao_loc = nullptr, const double *__restrict__ gamma = nullptr, int nao = 0)
+    const int *__restrict__ ao_loc = nullptr, const double *__restrict__ gamma = nullptr, int nao = 0,
+    double *__restrict__ full = nullptr)
 {
     extern __shared__ double smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     double *wsm = smem + warp * smem_warp;
     S2klOut so = {};
     so.gamma = gamma;
+    so.out = full;                 // MODE_FULL output
     so.nao = nao;
     constexpr int NC = D ? 3 : 1;
     constexpr int NOUT = MODE == MODE_QSUM ? 2 * NC : NC;
@@ -1225,7 +1273,8 @@ __global__ void __launch_bounds__(kWarps * 32, 2) eri_qsum_kernel(
         else
             eri_quartet<D, MODE, LOW>(atm, bas, env, ao_loc, s.x, s.y, s.z, s.w, wsm, smem_warp, so, acc, lane);
         if (lane == 0)
-            for (int c = 0; c < NOUT; c++) qsum[q * NOUT + c] = acc[c];
+            for (int c = 0; c < NOUT; c++)
+                if (MODE != MODE_FULL) qsum[q * NOUT + c] = acc[c];
     }
 }
 
@@ -1262,11 +1311,13 @@ template <int D, bool LOW, int MODE = MODE_QSUM>
 __global__ void __launch_bounds__(kHeavyThreads, 1) eri_qsum_heavy_kernel(
     const int *__restrict__ atm, const int *__restrict__ bas, const double *__restrict__ env,
     const int4 *__restrict__ quartets, long long nq, double *__restrict__ qsum, int smem_doubles,
-    const int *__restrict__ ao_loc = nullptr, const double *__restrict__ gamma = nullptr, int nao = 0)
+    const int *__restrict__ ao_loc = nullptr, const double *__restrict__ gamma = nullptr, int nao = 0,
+    double *__restrict__ full = nullptr)
 {
     extern __shared__ double smem[];
     S2klOut so = {};
     so.gamma = gamma;
+    so.out = full;                 // MODE_FULL output
     so.nao = nao;
     constexpr int NC = D ? 3 : 1;
     constexpr int NOUT = MODE == MODE_QSUM ? 2 * NC : NC;
@@ -1278,11 +1329,11 @@ __global__ void __launch_bounds__(kHeavyThreads, 1) eri_qsum_heavy_kernel(
                            bas[s.z * CB_BAS_SLOTS + CB_ANG_OF], bas[s.w * CB_BAS_SLOTS + CB_ANG_OF], h,
                            256 * kHcCtaMaxJ, smem_doubles, true)) {
             eri_quartet_hc_cta<D, MODE>(atm, bas, env, ao_loc, s.x, s.y, s.z, s.w, h, smem, smem_doubles, so,
-                                        qsum + q * NOUT);
+                                        MODE == MODE_FULL ? nullptr : qsum + q * NOUT);
             continue;
         }
         eri_quartet_cta<D, MODE, LOW>(atm, bas, env, ao_loc, s.x, s.y, s.z, s.w, smem, smem_doubles, so,
-                                      qsum + q * NOUT);
+                                      MODE == MODE_FULL ? nullptr : qsum + q * NOUT);
     }
 }
 
@@ -1594,6 +1645,48 @@ int ccsd_b200_eri_ip1_contract(const int32_t *atm, const int32_t *bas, const dou
     }
     segment_sum3_kernel<<<nseg, 256, 0, st>>>(qwork, seg, out);
     return check_launch("segment_sum3_kernel");
+}
+
+int ccsd_b200_eri_full_cart(const int32_t *atm, const int32_t *bas, const double *env, const int32_t *ao_loc,
+                            int nao, const int32_t *quartets, long long nq, int lmax, double *out, void *stream)
+{
+    if (!atm || !bas || !env || !ao_loc || nao <= 0 || !quartets || nq < 0 || lmax < 0 || !out) {
+        set_error("ccsd_b200_eri_full_cart: invalid argument");
+        return CCSD_B200_ERR_ARG;
+    }
+    if (lmax > CB_LMAX) {
+        set_error("ccsd_b200_eri_full_cart: l = %d > %d is not supported", lmax, CB_LMAX);
+        return CCSD_B200_ERR_UNSUPPORTED;
+    }
+    if (nq == 0) return CCSD_B200_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc;
+    const int sw = smem_per_warp(lmax, 0);
+    const size_t smem = (size_t)sw * kWarps * sizeof(double);
+    long long grid = (nq + kWarps - 1) / kWarps;
+    const long long gmax = (long long)num_sms() * 16;
+    if (grid > gmax) grid = gmax;
+    const int4 *q4 = reinterpret_cast<const int4 *>(quartets);
+    AuxStream *aux = nullptr;
+    if ((rc = aux_stream(&aux))) return rc;
+    cudaEventRecord(aux->fork, st);
+    cudaStreamWaitEvent(aux->s, aux->fork, 0);
+    const int hd = heavy_smem_doubles(lmax, 0);
+    const size_t hsmem = (size_t)hd * sizeof(double);
+    const long long hg = nq < (long long)num_sms() ? nq : (long long)num_sms();
+#define CB_LAUNCH_FULL(LOWV)                                                                                      \
+    if ((rc = prepare_kernel(eri_qsum_heavy_kernel<0, LOWV, MODE_FULL>, hsmem))) return rc;                       \
+    eri_qsum_heavy_kernel<0, LOWV, MODE_FULL><<<(int)hg, kHeavyThreads, hsmem, aux->s>>>(                        \
+        atm, bas, env, q4, nq, nullptr, hd, ao_loc, nullptr, nao, out);                                         \
+    if ((rc = check_launch("eri_qsum_heavy_kernel<full>"))) return rc;                                            \
+    cudaEventRecord(aux->join, aux->s);                                                                            \
+    if ((rc = prepare_kernel(eri_qsum_kernel<0, LOWV, MODE_FULL>, smem))) return rc;                              \
+    eri_qsum_kernel<0, LOWV, MODE_FULL><<<(int)grid, kWarps * 32, smem, st>>>(atm, bas, env, q4, nq, nullptr, sw,   \
+                                                                             ao_loc, nullptr, nao, out);
+    if (lmax <= 2) { CB_LAUNCH_FULL(true) } else { CB_LAUNCH_FULL(false) }
+#undef CB_LAUNCH_FULL
+    cudaStreamWaitEvent(st, aux->join, 0);
+    return check_launch("eri_qsum_kernel<full>");
 }
 
 int ccsd_b200_cart2sph_s2kl(const double *cart, double *tmp, double *out, int ncomp, int nfc, int naoc, int nfs,

@@ -1,8 +1,8 @@
 """Closed-shell Hartree-Fock on the GPU (the SCF the reference runs in PySCF on
 the CPU, examples/h2o_ccsd_grad.py:118-121).
 
-ERIs come from :func:`compute_int2e_gpu` over all shells and stay resident as
-a dense (nao,)*4 FP64 tensor (that fits HBM for every molecule of the
+ERIs come from :func:`full_eri_gpu` (each unique shell quartet computed once)
+and stay resident as a dense (nao,)*4 FP64 tensor (that fits HBM for every molecule of the
 configurations: (H2O)6/cc-pVDZ, nao = 144, is 3.4 GB).  J/K, DIIS and the
 eigen-solves are FP64 on the device.  The object exposes the attributes the
 CCSD gradient reads from a PySCF RHF: mol, mo_energy, mo_coeff, mo_occ, e_tot,
@@ -12,19 +12,52 @@ import numpy as np
 import torch
 
 from . import _native
-from .cuda.int2e_gpu import compute_int2e_gpu
+from .cuda.basis import _check_mol, get_basis_cached, upload_geometry
 from .int1e import intor1e
 
 
+def unique_quartets(topo):
+    """int32 (nq, 4) device list of the unique decontracted-shell quartets
+    (I >= J, K >= L, pair(IJ) >= pair(KL)), L-class ordered; cached."""
+    q = topo.__dict__.get("_unique_quartets")
+    if q is None:
+        nb = topo.dc_nbas
+        i, j = np.tril_indices(nb)
+        P, Q = np.tril_indices(len(i))
+        quart = np.stack([i[P], j[P], i[Q], j[Q]], 1).astype(np.int32)
+        l = topo.dc_bas[:, 1].astype(np.int64)[quart]
+        key = ((l[:, 0] * 5 + l[:, 1]) * 5 + l[:, 2]) * 5 + l[:, 3]
+        quart = quart[np.argsort(key, kind="stable")]
+        q = torch.from_numpy(np.ascontiguousarray(quart)).to(topo.device)
+        topo._unique_quartets = q
+    return q
+
+
 def full_eri_gpu(mol):
-    """(nao,)*4 chemist-notation ERI tensor on the GPU, native basis."""
-    s2kl = compute_int2e_gpu(mol, 0, mol.nbas)
-    n = s2kl.shape[0]
-    k, l = torch.tril_indices(n, n, device=s2kl.device)
-    g = torch.empty((n, n, n, n), dtype=torch.float64, device=s2kl.device)
-    g[:, :, k, l] = s2kl
-    g[:, :, l, k] = s2kl
-    return g
+    """(nao,)*4 chemist-notation ERI tensor on the GPU, native basis.
+
+    Each unique shell quartet is computed once (``ccsd_b200_eri_full_cart``
+    writes all eight index orders); a spherical basis is reached by four
+    dense transforms of the Cartesian tensor."""
+    _native.require_cuda()
+    if not _check_mol(mol):
+        raise ValueError("shells with l > 4 are not supported (nroots > 9)")
+    dev = torch.device("cuda", torch.cuda.current_device())
+    topo = get_basis_cached(mol, dev)
+    atm, env = upload_geometry(mol, dev)
+    q = unique_quartets(topo)
+    n = topo.nao_cart
+    g = torch.empty((n, n, n, n), dtype=torch.float64, device=dev)
+    _native.call("ccsd_b200_eri_full_cart", _native.ptr(atm), _native.ptr(topo.bas_dev), _native.ptr(env),
+                 _native.ptr(topo.ao_loc_dev), n, _native.ptr(q), int(q.shape[0]), topo.lmax, _native.ptr(g),
+                 _native.stream())
+    if mol.cart:
+        return g
+    T = torch.as_tensor(topo.sph()["C"], dtype=torch.float64, device=dev)      # (ncart, nsph)
+    g = torch.einsum("ap,abcd->pbcd", T, g)
+    g = torch.einsum("bq,pbcd->pqcd", T, g)
+    g = torch.einsum("cr,pqcd->pqrd", T, g)
+    return torch.einsum("ds,pqrd->pqrs", T, g).contiguous()
 
 
 class RHF:

@@ -122,6 +122,19 @@ int ccsd_b200_int1e_cart(int op, const int32_t *atm, int natm, const int32_t *ba
 int ccsd_b200_fp64_fma_probe(double *out, int blocks, int iters, void *stream);
 
 /*
+ * Dense Cartesian ERI tensor from the unique shell quartets: for every
+ * quartet (I, J, K, L) of `quartets` (decontracted shells; the caller lists
+ * each unique quartet once, e.g. I >= J, K >= L, IJ >= KL) the (IJ|KL) block
+ * is computed once and written to all eight index orders of
+ * out[nao][nao][nao][nao] (FP64, Cartesian AO order of ao_loc).  Replaces the
+ * repeated s2kl blocks (all I, all J) that the reference's SCF/Imat path
+ * requests (ref: ccsd_gpu/cuda/int2e_gpu.py:186-215 called per i-shell
+ * block, ccsd_gpu/gpu_ccsd_grad.py:436-441) when the whole tensor is needed.
+ */
+int ccsd_b200_eri_full_cart(const int32_t *atm, const int32_t *bas, const double *env, const int32_t *ao_loc,
+                            int nao, const int32_t *quartets, long long nq, int lmax, double *out, void *stream);
+
+/*
  * Two-electron part of the nuclear gradient without storing ERI derivatives:
  * for every shell quartet q = (I, J, K, L) of `quartets` (decontracted shells,
  * K >= L, derivative on I) the (dI J|K L) block is built shell quartet by shell

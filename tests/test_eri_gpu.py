@@ -105,3 +105,25 @@ def test_invalid_arguments_are_rejected_on_host():
         x = torch.zeros(8, dtype=torch.float64, device="cuda")
         _native.call("ccsd_b200_eri_s2kl_cart", 0, _native.ptr(x), _native.ptr(x), _native.ptr(x), 1,
                      _native.ptr(x), 0, 1, 1, 5, None, 0, _native.ptr(x), None)
+
+
+@pytest.mark.parametrize("cart", [True, False])
+def test_dense_eri_from_unique_quartets_matches_s2kl_and_oracle(cart):
+    """full_eri_gpu computes each unique shell quartet once and writes all 8
+    index orders: it must equal the s2kl path unpacked, and the oracle."""
+    from ccsd_gpu_b200 import compute_int2e_gpu
+    from ccsd_gpu_b200.gto import M
+    from ccsd_gpu_b200.scf import full_eri_gpu
+    for atom in ("O 0 0 0; H 0 0.757 0.587; H 0 -0.757 0.587",
+                 "C 0 0 0; O 0 0 1.2; H 0.9 0 -0.5; H -0.9 0 -0.5"):
+        mol = M(atom=atom, basis="cc-pvdz", cart=cart)
+        g = _np(full_eri_gpu(mol))
+        n = g.shape[0]
+        ref = _full_tensor(_np(compute_int2e_gpu(mol, 0, mol.nbas)), n)
+        assert np.abs(g - ref).max() <= 1e-12 * np.abs(ref).max()
+        # equal shells write both (i, j) orders: equal up to the last bits
+        assert np.abs(g - g.transpose(1, 0, 2, 3)).max() <= 1e-14 * np.abs(g).max()
+        assert np.abs(g - g.transpose(2, 3, 0, 1)).max() <= 1e-14 * np.abs(g).max()
+        if atom.startswith("O"):
+            k, l = np.tril_indices(n)
+            assert block_close(g[:, :, k, l], oracle_eri.s2kl(mol, 0, mol.nbas, 0))
