@@ -30,7 +30,7 @@ SIGNATURES = {
     "ccsd_b200_cart2sph_s2kl_noalloc": (_c_int, [_vp, _vp, _c_int, _c_int, _c_int, _c_int, _c_int,
                                                  _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "ccsd_b200_split_pack": (_c_int, [_c_int, _vp, _vp, _vp, _c_dbl, _vp, _vp, _vp, _c_dbl, _c_int, _c_int,
-                                      _c_int, _c_int, _vp, _vp, _vp]),
+                                      _c_int, _c_int, _vp, _vp, _c_int, _vp]),
     "ccsd_b200_eri_full_cart": (_c_int, [_vp, _vp, _vp, _vp, _c_int, _vp, _c_ll, _c_int, _vp, _vp]),
     "ccsd_b200_eri_ip1_contract": (_c_int, [_vp, _vp, _vp, _vp, _c_int, _vp, _vp, _c_ll, _vp, _c_int, _c_int, _vp,
                                             _vp, _vp]),

@@ -182,8 +182,13 @@ def _pack_new(terms, sub, rows_idx, k_idx, shape_map, kind, rows_pad, k_pad, dev
     else:
         p2 = (_native.ptr(None), _native.ptr(None), _native.ptr(None), 0.0)
     STATS["launches"] += 1
+    # transposing gather: the source is contiguous along the packed rows
+    st = dict(zip(sub, t1.stride()))
+    sr = st.get(rows_idx[-1], 0) if rows_idx else 0
+    sk = st.get(k_idx[-1], 0) if k_idx else 0
+    rowfast = int(sr == 1 and sk != 1)
     _native.call("ccsd_b200_split_pack", kind, _native.ptr(t1), _native.ptr(o1r), _native.ptr(o1k), c1, *p2,
-                 rows, K, rows_pad, k_pad, _native.ptr(hi), _native.ptr(lo), stream)
+                 rows, K, rows_pad, k_pad, _native.ptr(hi), _native.ptr(lo), rowfast, stream)
     return hi, lo
 
 

@@ -381,34 +381,72 @@ __global__ void splitk_reduce_kernel(const double *__restrict__ partial, int ksp
 // dst row r, column k  <-  c1 * src1[o1r[r] + o1k[k]] + c2 * src2[o2r[r] + o2k[k]]
 // (second term optional), split into hi + lo of the MMA input type.
 template <int KIND>
-__global__ void split_pack_kernel(const double *__restrict__ src1, const long long *__restrict__ o1r,
-                                  const long long *__restrict__ o1k, double c1, const double *__restrict__ src2,
-                                  const long long *__restrict__ o2r, const long long *__restrict__ o2k, double c2,
-                                  int rows, int K, int rows_pad, int k_pad, void *__restrict__ hi,
-                                  void *__restrict__ lo)
+__device__ __forceinline__ void split_store(void *__restrict__ hi, void *__restrict__ lo, long long e, double x)
 {
-    const long long total = (long long)rows_pad * k_pad;
-    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
-         e += (long long)gridDim.x * blockDim.x) {
-        const int r = (int)(e / k_pad), k = (int)(e - (long long)r * k_pad);
-        double x = 0.0;
-        if (r < rows && k < K) {
-            x = c1 * src1[o1r[r] + o1k[k]];
-            if (src2) x = fma(c2, src2[o2r[r] + o2k[k]], x);
-        }
-        if (KIND == KIND_TF32) {
-            uint32_t h, l;
-            const float xf = (float)x;
-            asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(xf));
-            const float rest = (float)(x - (double)__uint_as_float(h));
-            asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(l) : "f"(rest));
-            reinterpret_cast<uint32_t *>(hi)[e] = h;
-            reinterpret_cast<uint32_t *>(lo)[e] = l;
+    if (KIND == KIND_TF32) {
+        uint32_t h, l;
+        const float xf = (float)x;
+        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(xf));
+        const float rest = (float)(x - (double)__uint_as_float(h));
+        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(l) : "f"(rest));
+        reinterpret_cast<uint32_t *>(hi)[e] = h;
+        reinterpret_cast<uint32_t *>(lo)[e] = l;
+    } else {
+        const __nv_bfloat16 h = __double2bfloat16(x);
+        const __nv_bfloat16 l = __double2bfloat16(x - (double)__bfloat162float(h));
+        reinterpret_cast<__nv_bfloat16 *>(hi)[e] = h;
+        reinterpret_cast<__nv_bfloat16 *>(lo)[e] = l;
+    }
+}
+
+__device__ __forceinline__ double pack_value(const double *__restrict__ src1, const long long *__restrict__ o1r,
+                                             const long long *__restrict__ o1k, double c1,
+                                             const double *__restrict__ src2, const long long *__restrict__ o2r,
+                                             const long long *__restrict__ o2k, double c2, int r, int k, int rows,
+                                             int K)
+{
+    if (r >= rows || k >= K) return 0.0;
+    double x = c1 * src1[o1r[r] + o1k[k]];
+    if (src2) x = fma(c2, src2[o2r[r] + o2k[k]], x);
+    return x;
+}
+
+// 32 x 32 tiles, 32 x 8 threads.  The packed array is K-major, so writes go
+// with lanes along k.  ROWFAST: the source is contiguous along the packed
+// rows (a transposing gather), so lanes read along rows and the tile turns
+// through shared memory; otherwise lanes read and write along k directly.
+template <int KIND, bool ROWFAST>
+__global__ void __launch_bounds__(256) split_pack_kernel(
+    const double *__restrict__ src1, const long long *__restrict__ o1r, const long long *__restrict__ o1k, double c1,
+    const double *__restrict__ src2, const long long *__restrict__ o2r, const long long *__restrict__ o2k, double c2,
+    int rows, int K, int rows_pad, int k_pad, void *__restrict__ hi, void *__restrict__ lo)
+{
+    __shared__ double tile[32][33];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int k0 = blockIdx.x * 32;
+    const int nrt = (rows_pad + 31) / 32;
+    for (int rt = blockIdx.y; rt < nrt; rt += gridDim.y) {
+        const int r0 = rt * 32;
+        if (ROWFAST) {
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+                tile[ty + 8 * i][tx] = pack_value(src1, o1r, o1k, c1, src2, o2r, o2k, c2, r0 + tx, k0 + ty + 8 * i,
+                                                  rows, K);
+            __syncthreads();
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const int r = r0 + ty + 8 * i, k = k0 + tx;
+                if (r < rows_pad && k < k_pad) split_store<KIND>(hi, lo, (long long)r * k_pad + k, tile[tx][ty + 8 * i]);
+            }
+            __syncthreads();
         } else {
-            const __nv_bfloat16 h = __double2bfloat16(x);
-            const __nv_bfloat16 l = __double2bfloat16(x - (double)__bfloat162float(h));
-            reinterpret_cast<__nv_bfloat16 *>(hi)[e] = h;
-            reinterpret_cast<__nv_bfloat16 *>(lo)[e] = l;
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const int r = r0 + ty + 8 * i, k = k0 + tx;
+                if (r < rows_pad && k < k_pad)
+                    split_store<KIND>(hi, lo, (long long)r * k_pad + k,
+                                      pack_value(src1, o1r, o1k, c1, src2, o2r, o2k, c2, r, k, rows, K));
+            }
         }
     }
 }
@@ -500,7 +538,7 @@ int ccsd_b200_wait_probe(int *status, long long limit_ns, int code, void *stream
 
 int ccsd_b200_split_pack(int kind, const double *src1, const long long *o1r, const long long *o1k, double c1,
                          const double *src2, const long long *o2r, const long long *o2k, double c2, int rows, int K,
-                         int rows_pad, int k_pad, void *hi, void *lo, void *stream)
+                         int rows_pad, int k_pad, void *hi, void *lo, int rowfast, void *stream)
 {
     if ((kind != KIND_TF32 && kind != KIND_BF16) || !src1 || !o1r || !o1k || rows < 0 || K < 0 ||
         rows_pad < rows || k_pad < K || !hi || !lo || (src2 && (!o2r || !o2k)) ||
@@ -508,17 +546,19 @@ int ccsd_b200_split_pack(int kind, const double *src1, const long long *o1r, con
         set_error("ccsd_b200_split_pack: invalid argument");
         return CCSD_B200_ERR_ARG;
     }
-    const long long total = (long long)rows_pad * k_pad;
-    if (total == 0) return CCSD_B200_OK;
-    long long grid = (total + 255) / 256;
-    if (grid > 148 * 64) grid = 148 * 64;
+    if ((long long)rows_pad * k_pad == 0) return CCSD_B200_OK;
+    const int nrt = (rows_pad + 31) / 32;
+    dim3 grid((unsigned)((k_pad + 31) / 32), (unsigned)(nrt < 65535 ? nrt : 65535));
     cudaStream_t st = (cudaStream_t)stream;
-    if (kind == KIND_TF32)
-        split_pack_kernel<KIND_TF32><<<(int)grid, 256, 0, st>>>(src1, o1r, o1k, c1, src2, o2r, o2k, c2, rows, K,
-                                                                rows_pad, k_pad, hi, lo);
-    else
-        split_pack_kernel<KIND_BF16><<<(int)grid, 256, 0, st>>>(src1, o1r, o1k, c1, src2, o2r, o2k, c2, rows, K,
-                                                                rows_pad, k_pad, hi, lo);
+#define CB_PACK(KD, RF)                                                                                     \
+    split_pack_kernel<KD, RF><<<grid, 256, 0, st>>>(src1, o1r, o1k, c1, src2, o2r, o2k, c2, rows, K, rows_pad, \
+                                                    k_pad, hi, lo)
+    if (kind == KIND_TF32) {
+        if (rowfast) CB_PACK(KIND_TF32, true); else CB_PACK(KIND_TF32, false);
+    } else {
+        if (rowfast) CB_PACK(KIND_BF16, true); else CB_PACK(KIND_BF16, false);
+    }
+#undef CB_PACK
     return check_launch("split_pack_kernel");
 }
 

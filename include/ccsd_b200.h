@@ -171,6 +171,9 @@ int ccsd_b200_wait_probe(int *status, long long limit_ns, int code, void *stream
  * rows_pad >= rows; k_pad >= K and a multiple of 4 (TF32) / 8 (BF16), so
  * that every row starts on a 16-byte boundary.  No padding to the 128-row
  * GEMM tile is needed: the GEMM's TMA loads read zeros past the array.
+ * rowfast != 0 tells that src1 is contiguous along the packed rows (a
+ * transposing gather): the kernel then reads along rows and turns 32 x 32
+ * tiles through shared memory, so reads and writes are both coalesced.
  * The offset tables (int64, element units) express any strided or permuted
  * view of the FP64 operands.  Replaces the operand transposes/copies that
  * precede the CuPy einsum contractions of the Lambda and RDM builders
@@ -178,7 +181,7 @@ int ccsd_b200_wait_probe(int *status, long long limit_ns, int code, void *stream
  */
 int ccsd_b200_split_pack(int kind, const double *src1, const long long *o1r, const long long *o1k, double c1,
                          const double *src2, const long long *o2r, const long long *o2k, double c2, int rows,
-                         int K, int rows_pad, int k_pad, void *hi, void *lo, void *stream);
+                         int K, int rows_pad, int k_pad, void *hi, void *lo, int rowfast, void *stream);
 
 /*
  * Split-precision tensor-core contraction, step 2 (tcgen05 + TMA + TMEM):

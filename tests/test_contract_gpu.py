@@ -140,3 +140,18 @@ def test_tensor_route_on_tiny_and_ragged_shapes(mode, tol, monkeypatch):
         C.check_status()
         assert C.STATS["launches"] - n0 >= 3
         assert _rel(got, a @ b.T) < tol, (M, N, K)
+
+
+@pytest.mark.parametrize("mode,tol", [("tf32x3", 5e-6), ("bf16x3", 1e-4)])
+def test_transposing_gather_pack(mode, tol, monkeypatch):
+    """Operands stored contiguous along the packed rows (here A as (K, M) and
+    B as (K, N)) take the shared-memory transposing pack; ragged tile edges."""
+    import ccsd_gpu_b200.contract as C
+    monkeypatch.setattr(C, "SMALL_FLOPS", 0.0)
+    g = torch.Generator(device="cuda").manual_seed(8)
+    for M, N, K in [(333, 200, 129), (64, 1000, 300), (5, 7, 40)]:
+        a = torch.randn(K, M, dtype=torch.float64, device="cuda", generator=g)
+        b = torch.randn(K, N, dtype=torch.float64, device="cuda", generator=g)
+        got = C.contract("km,kn->mn", a, b, mode=mode)
+        C.check_status()
+        assert _rel(got, a.T @ b) < tol, (M, N, K)
