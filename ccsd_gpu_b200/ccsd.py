@@ -20,16 +20,22 @@ from .graphs import StepGraph
 from .gpu_ccsd_lambda import DIIS, DeviceEris, amplitude_norm_sq, solve_lambda_gpu
 
 
-def ao2mo_gpu(mf, mo_coeff=None):
-    """Chemist-notation MO blocks (PySCF ``_ChemistsERIs`` layout) on the GPU, FP64."""
+def ao2mo_gpu(mf, mo_coeff=None, frozen=0):
+    """Chemist-notation MO blocks (PySCF ``_ChemistsERIs`` layout) on the GPU, FP64.
+
+    ``frozen`` lowest orbitals are left out of the correlation space: the blocks
+    and the Fock matrix span the active orbitals only, the Fock matrix still
+    built from the full HF density."""
     C = torch.as_tensor(mf.mo_coeff if mo_coeff is None else mo_coeff, dtype=torch.float64,
                         device=mf.eri.device)
-    nocc = int((np.asarray(mf.mo_occ) > 0).sum())
+    nocc_all = int((np.asarray(mf.mo_occ) > 0).sum())
+    dm = 2 * C[:, :nocc_all] @ C[:, :nocc_all].T
+    C = C[:, frozen:]
+    nocc = nocc_all - frozen
     g = torch.einsum("pqrs,pi->iqrs", mf.eri, C)
     g = torch.einsum("iqrs,qj->ijrs", g, C)
     g = torch.einsum("ijrs,rk->ijks", g, C)
     g = torch.einsum("ijks,sl->ijkl", g, C)
-    dm = 2 * C[:, :nocc] @ C[:, :nocc].T
     fock = C.T @ (mf.get_hcore() + mf.get_veff(dm=dm)) @ C
     o, v = slice(0, nocc), slice(nocc, C.shape[1])
     e = SimpleNamespace(fock=fock, mo_energy=torch.diagonal(fock).clone(), oooo=g[o, o, o, o].contiguous(),
@@ -130,9 +136,13 @@ def energy_gpu(t1, t2, eris):
 
 
 class CCSD:
-    """PySCF-like closed-shell CCSD on the GPU (frozen core off)."""
+    """PySCF-like closed-shell CCSD on the GPU.
 
-    def __init__(self, mf, precision="tf32x3"):
+    ``frozen``: number of lowest (core) orbitals kept out of the correlation
+    treatment, as PySCF's integer ``frozen`` (ref: the reference's frozen-core
+    branches, ccsd_gpu/gpu_ccsd_grad.py:373-374,510-518)."""
+
+    def __init__(self, mf, precision="tf32x3", frozen=0):
         _native.require_cuda()
         self._scf = mf
         self.mol = mf.mol
@@ -156,14 +166,18 @@ class CCSD:
         self.t1 = self.t2 = self.l1 = self.l2 = None
         self.converged = self.converged_lambda = False
         self._eris = None
+        self.frozen = int(frozen or 0)
+        if not 0 <= self.frozen < int((np.asarray(self.mo_occ) > 0).sum()):
+            raise ValueError("frozen must leave at least one active occupied orbital")
 
     @property
     def nocc(self):
-        return int((np.asarray(self.mo_occ) > 0).sum())
+        """Active occupied orbitals."""
+        return int((np.asarray(self.mo_occ) > 0).sum()) - self.frozen
 
     def ao2mo(self, mo_coeff=None):
         if self._eris is None or mo_coeff is not None:
-            self._eris = ao2mo_gpu(self._scf, mo_coeff)
+            self._eris = ao2mo_gpu(self._scf, mo_coeff, self.frozen)
         return self._eris
 
     def kernel(self, t1=None, t2=None, eris=None):

@@ -188,11 +188,16 @@ def grad_elec_gpu(mycc, t1, t2, l1, l2, atmlst=None, verbose=None):
     e = _t(mf.mo_energy, dev)
     nao, nmo = C.shape
     nocc = int((np.asarray(mf.mo_occ) > 0).sum())
+    # frozen core: the amplitudes span occupied orbitals nf..nocc-1 (ref:
+    # ccsd_gpu/gpu_ccsd_grad.py:373-374); no frozen virtuals
+    nf = nocc - int(np.shape(t1)[0])
+    if nf < 0 or int(np.shape(t1)[1]) != nmo - nocc:
+        raise ValueError("amplitudes do not match the SCF orbitals (only frozen core orbitals are supported)")
     Co, Cv = C[:, :nocc], C[:, nocc:]
     eri = mf.eri
     doo, dov, dvo, dvv = _gamma1_intermediates_gpu(mycc, t1, t2, l1, l2)
     d2 = _gamma2_intermediates_gpu(mycc, t1, t2, l1, l2)
-    dm2 = _rdm2_ao(d2, C)
+    dm2 = _rdm2_ao(d2, C[:, nf:])
     del d2
     P = 2 * Co @ Co.T
     atmlst = range(mol.natm) if atmlst is None else atmlst
@@ -202,8 +207,14 @@ def grad_elec_gpu(mycc, t1, t2, l1, l2, atmlst=None, verbose=None):
     S = mf.get_ovlp()
     Imat = -(C.T @ Imat @ S @ C)
     dm1mo = torch.zeros((nmo, nmo), dtype=torch.float64, device=dev)
-    dm1mo[:nocc, :nocc] = doo + doo.T
+    dm1mo[nf:nocc, nf:nocc] = doo + doo.T
     dm1mo[nocc:, nocc:] = dvv + dvv.T
+    if nf:
+        # frozen-active occupied block of the relaxed density
+        # (ref: ccsd_gpu/gpu_ccsd_grad.py:510-518)
+        dco = Imat[:nf, nf:nocc] / (e[:nf, None] - e[None, nf:nocc])
+        dm1mo[:nf, nf:nocc] = dco
+        dm1mo[nf:nocc, :nf] = dco.T
     dm1 = C @ dm1mo @ C.T
     vhf = mf.get_veff(dm=dm1) * 2
     Xvo = Cv.T @ vhf @ Co + Imat[:nocc, nocc:].T - Imat[nocc:, :nocc]
@@ -309,7 +320,8 @@ def compute_ml_ccsd_forces_gpu(mf, t1, t2, l1, l2, precision="tf32x3"):
 
     As in the reference this is the gradient (not its negative)."""
     from .ccsd import CCSD
-    mycc = CCSD(mf, precision=precision)
+    nf = int((np.asarray(mf.mo_occ) > 0).sum()) - int(np.shape(t1)[0])     # frozen core from the shapes
+    mycc = CCSD(mf, precision=precision, frozen=nf)
     mycc.t1, mycc.t2, mycc.l1, mycc.l2 = t1, t2, l1, l2
     mycc.converged = mycc.converged_lambda = True
     de = grad_elec_gpu(mycc, t1, t2, l1, l2)
@@ -328,12 +340,12 @@ class CCSDEnergy(torch.autograd.Function):
     """
 
     @staticmethod
-    def forward(ctx, coords, mol, precision="tf32x3"):
+    def forward(ctx, coords, mol, precision="tf32x3", frozen=0):
         from .ccsd import CCSD
         from .scf import RHF
         m = mol.copy().set_geom_(coords.detach().cpu().numpy())
         mf = RHF(m).run()
-        cc = CCSD(mf, precision=precision)
+        cc = CCSD(mf, precision=precision, frozen=frozen)
         cc.kernel()
         ctx.cc = cc
         return torch.tensor(cc.e_tot, dtype=torch.float64, device=coords.device)
@@ -341,4 +353,4 @@ class CCSDEnergy(torch.autograd.Function):
     @staticmethod
     def backward(ctx, gout):
         g = ctx.cc.nuc_grad_method().kernel()
-        return gout * torch.as_tensor(g, dtype=torch.float64, device=gout.device), None, None
+        return gout * torch.as_tensor(g, dtype=torch.float64, device=gout.device), None, None, None
