@@ -84,8 +84,11 @@ def update_amps_gpu(t1, t2, eris, mode="tf32x3", level_shift=0.0):
     E("kdac,ikcd->ia", Xovvv, t2, out=t1n, beta=1.0)
     E("lcki,klac->ia", Yovoo, t2, out=t1n, alpha=-1.0, beta=1.0)
     # T2
-    tmp2 = ovvv.permute(1, 3, 0, 2) - torch.einsum("kibc,ka->abic", oovv, t1)
-    tmp = E("abic,jc->ijab", tmp2, t1)
+    # (ovvv^T - oovv t1) t1 without the o v^3 intermediate: the second
+    # product goes through X[k,i,b,j] = sum_c oovv[k,i,b,c] t1[j,c] (o^3 v)
+    tmp = E("iacb,jc->ijab", ovvv, t1)
+    xk = E("kibc,jc->kibj", oovv, t1)
+    E("kibj,ka->ijab", xk, t1, out=tmp, alpha=-1.0, beta=1.0)
     t2n = tmp + tmp.permute(1, 0, 3, 2)
     tmp2 = E("kcai,jc->akij", ovvo, t1)
     tmp2 += ovoo.permute(1, 3, 0, 2)

@@ -198,7 +198,7 @@ def _pack_new(terms, sub, rows_idx, k_idx, shape_map, kind, rows_pad, k_pad, dev
 # LOW_INTENSITY_MAX_K: such shapes are bound by HBM, not by the tensor cores.
 # Long, skinny reductions stay on the split-K tensor-core route (cuBLAS
 # parallelises them poorly, and their large operands stay packed in the cache).
-LOW_INTENSITY_K = 32
+LOW_INTENSITY_K = 16
 LOW_INTENSITY_FLOP_PER_BYTE = 12.0
 LOW_INTENSITY_MAX_K = 1024
 # below this many flops a contraction is launch-bound: one cuBLAS call beats
@@ -283,8 +283,13 @@ def contract(spec, a, b, out=None, alpha=1.0, beta=0.0, mode="tf32x3", stream=No
     K = int(np.prod([shape_map[i] for i in k_idx])) if k_idx else 1
     if M == 0 or N == 0:
         return out
+    # a registered constant operand stays packed in the cache, while the FP64
+    # route would re-gather (permute-copy) it on every call
+    big = ta if M >= N else tb
+    big_cached = all(_is_const(t) for _, t in big)
     if K <= LOW_INTENSITY_K or 2.0 * M * N * K < SMALL_FLOPS or (
-            K <= LOW_INTENSITY_MAX_K and 2.0 * M * N * K < LOW_INTENSITY_FLOP_PER_BYTE * 8.0 * (M * K + N * K + M * N)):
+            not big_cached and K <= LOW_INTENSITY_MAX_K and
+            2.0 * M * N * K < LOW_INTENSITY_FLOP_PER_BYTE * 8.0 * (M * K + N * K + M * N)):
         # memory-bound shape: FP64 through cuBLAS moves fewer bytes than the
         # split/pack/tensor-core route and is exact to FP64
         return _fp64_contract(spec, ta, tb, shape_map, out, alpha, beta)

@@ -340,12 +340,13 @@ class CCSDEnergy(torch.autograd.Function):
     """
 
     @staticmethod
-    def forward(ctx, coords, mol, precision="tf32x3", frozen=0):
+    def forward(ctx, coords, mol, precision="tf32x3", frozen=0, polish=True):
         from .ccsd import CCSD
         from .scf import RHF
         m = mol.copy().set_geom_(coords.detach().cpu().numpy())
         mf = RHF(m).run()
         cc = CCSD(mf, precision=precision, frozen=frozen)
+        cc.t_polish = cc.lambda_polish = bool(polish)
         cc.kernel()
         ctx.cc = cc
         return torch.tensor(cc.e_tot, dtype=torch.float64, device=coords.device)
@@ -353,4 +354,4 @@ class CCSDEnergy(torch.autograd.Function):
     @staticmethod
     def backward(ctx, gout):
         g = ctx.cc.nuc_grad_method().kernel()
-        return gout * torch.as_tensor(g, dtype=torch.float64, device=gout.device), None, None, None
+        return gout * torch.as_tensor(g, dtype=torch.float64, device=gout.device), None, None, None, None

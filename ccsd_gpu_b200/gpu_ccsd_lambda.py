@@ -232,31 +232,44 @@ def amplitude_norm_sq(d1, d2):
 
 
 class DIIS:
-    """Pulay extrapolation on the device in FP64; error vector = x_new - x_old."""
+    """Pulay extrapolation on the device in FP64; error vector = x_new - x_old.
+
+    The vectors live in two preallocated ring buffers and the Gram matrix of
+    the error vectors is kept up to date, so one update reads the stored
+    errors once (one GEMV for the new row of the Gram matrix) and the stored
+    vectors once (one GEMV for the extrapolation): no stacking copies and no
+    Gram GEMM over the whole subspace per iteration."""
 
     def __init__(self, space=6):
         self.space = space
-        self.xs, self.es = [], []
+        self.count = 0
+        self.xbuf = self.ebuf = self.gram = None
 
     def update(self, x, err):
-        self.xs.append(x)
-        self.es.append(err)
-        if len(self.xs) > self.space:
-            self.xs.pop(0)
-            self.es.pop(0)
-        n = len(self.xs)
+        x, err = x.reshape(-1), err.reshape(-1)
+        if self.xbuf is None:
+            self.xbuf = torch.empty((self.space, x.numel()), dtype=torch.float64, device=x.device)
+            self.ebuf = torch.empty_like(self.xbuf)
+            self.gram = torch.zeros((self.space, self.space), dtype=torch.float64, device=x.device)
+        slot = self.count % self.space
+        self.count += 1
+        n = min(self.count, self.space)
+        self.xbuf[slot].copy_(x)
+        self.ebuf[slot].copy_(err)
+        row = torch.mv(self.ebuf[:n], self.ebuf[slot])
+        self.gram[slot, :n] = row
+        self.gram[:n, slot] = row
         if n < 2:
             return x
+        G = self.gram[:n, :n]
         B = torch.empty((n + 1, n + 1), dtype=torch.float64, device=x.device)
-        E = torch.stack(self.es)
-        G = E @ E.T
         B[:n, :n] = G / G.diagonal().abs().max().clamp_min(1e-300)
         B[n, :n] = B[:n, n] = -1.0
         B[n, n] = 0.0
         rhs = torch.zeros(n + 1, 1, dtype=torch.float64, device=x.device)
         rhs[n] = -1.0
         c = torch.linalg.lstsq(B, rhs).solution[:n, 0]
-        return (c[:, None] * torch.stack(self.xs)).sum(0)
+        return torch.mv(self.xbuf[:n].T, c)
 
 
 MIXED_FLOOR = 1e-6     # update norm below which split-precision iterations stop helping
