@@ -963,9 +963,13 @@ __device__ __forceinline__ void eri_quartet_hc_cta(const int *__restrict__ atm, 
                                                  threadIdx.x, cap);
 }
 
-// Quartets whose Cartesian block has more functions than this go to the
-// CTA-cooperative kernel; smaller ones are one warp each.
+// Quartets whose Cartesian block has more functions than heavy_nf(D) go to
+// the CTA-cooperative kernel; smaller ones are one warp each.  Measured on the
+// 2^18-quartet benchmark set: int2e is fastest with the (dd|dp)-class blocks
+// (648 functions) on warps, int2e_ip1 with them on CTAs (119 -> 89 ms).
 static constexpr int kHeavyNf = 1000;
+static constexpr int kHeavyNfIp1 = 500;
+__host__ __device__ constexpr int heavy_nf(int D) { return D ? kHeavyNfIp1 : kHeavyNf; }
 
 __device__ __forceinline__ int quartet_nf(const int *__restrict__ bas, int i, int j, int k, int l)
 {
@@ -1223,7 +1227,7 @@ __global__ void __launch_bounds__(kWarps * 32, 2) eri_s2kl_kernel(
         int ksh, lsh;
         decode_pair(q - ij * npairs, ksh, lsh);
         const int ish = ish0 + (int)(ij / nbas), jsh = (int)(ij % nbas);
-        if (quartet_nf(bas, ish, jsh, ksh, lsh) > kHeavyNf) continue;
+        if (quartet_nf(bas, ish, jsh, ksh, lsh) > heavy_nf(D)) continue;
         if (LOW) {
             HcPlan h;
             if (hc_plan(D, bas[ish * CB_BAS_SLOTS + CB_ANG_OF], bas[jsh * CB_BAS_SLOTS + CB_ANG_OF],
@@ -1263,7 +1267,7 @@ __global__ void __launch_bounds__(kWarps * 32, 2) eri_qsum_kernel(
     for (long long t = t0 + warp; t < t1; t += kWarps) {
         const long long q = nq - 1 - t;
         const int4 s = quartets[q];
-        if (quartet_nf(bas, s.x, s.y, s.z, s.w) > kHeavyNf) continue;
+        if (quartet_nf(bas, s.x, s.y, s.z, s.w) > heavy_nf(D)) continue;
         double acc[NOUT];
         for (int c = 0; c < NOUT; c++) acc[c] = 0.0;
         HcPlan h;
@@ -1323,7 +1327,7 @@ __global__ void __launch_bounds__(kHeavyThreads, 1) eri_qsum_heavy_kernel(
     constexpr int NOUT = MODE == MODE_QSUM ? 2 * NC : NC;
     for (long long q = blockIdx.x; q < nq; q += gridDim.x) {
         const int4 s = quartets[q];
-        if (quartet_nf(bas, s.x, s.y, s.z, s.w) <= kHeavyNf) continue;
+        if (quartet_nf(bas, s.x, s.y, s.z, s.w) <= heavy_nf(D)) continue;
         HcPlan h;
         if (LOW && hc_plan(D, bas[s.x * CB_BAS_SLOTS + CB_ANG_OF], bas[s.y * CB_BAS_SLOTS + CB_ANG_OF],
                            bas[s.z * CB_BAS_SLOTS + CB_ANG_OF], bas[s.w * CB_BAS_SLOTS + CB_ANG_OF], h,

@@ -6,14 +6,16 @@ from .. import _native
 from .basis import _check_mol, get_basis_cached, upload_geometry
 
 
-HEAVY_NF = 1000   # Cartesian functions per quartet above which the CTA kernel is used
+# Cartesian functions per quartet above which the CTA kernel is used: int2e,
+# int2e_ip1 (the same thresholds as heavy_nf() in csrc/eri.cu)
+HEAVY_NF = {0: 1000, 1: 500}
 
 
-def heavy_quartets(topo, d0, d1):
-    """(n, 4) int32 device list of the block's quartets with more than HEAVY_NF functions."""
+def heavy_quartets(topo, d0, d1, deriv=0):
+    """(n, 4) int32 device list of the block's quartets with more than HEAVY_NF[deriv] functions."""
     cache = topo.__dict__.setdefault("_heavy", {})
-    if (d0, d1) in cache:
-        return cache[(d0, d1)]
+    if (d0, d1, deriv) in cache:
+        return cache[(d0, d1, deriv)]
     l = topo.dc_bas[:, 1].astype(np.int64)
     nc = (l + 1) * (l + 2) // 2
     nb = topo.dc_nbas
@@ -22,11 +24,11 @@ def heavy_quartets(topo, d0, d1):
     i = np.arange(d0, d1)
     j = np.arange(nb)
     nij = (nc[i][:, None] * nc[j][None, :]).ravel()
-    ij, pp = np.nonzero(nij[:, None] * nkl[None, :] > HEAVY_NF)
+    ij, pp = np.nonzero(nij[:, None] * nkl[None, :] > HEAVY_NF[deriv])
     q = np.stack([i[ij // nb], j[ij % nb], k[pp], ll[pp]], 1).astype(np.int32)
     order = np.argsort(-(nij[ij] * nkl[pp]), kind="stable")     # heaviest first
     dev = torch.from_numpy(np.ascontiguousarray(q[order]).reshape(-1, 4)).to(topo.device)
-    cache[(d0, d1)] = dev
+    cache[(d0, d1, deriv)] = dev
     return dev
 
 
@@ -48,7 +50,7 @@ def compute_s2kl(mol, b0, b1, deriv, stream=None):
     ncomp = 3 if deriv else 1
     st = _native.stream(stream)
     cart = torch.empty((ncomp, nfc, naoc, npc), dtype=torch.float64, device=dev)
-    hq = heavy_quartets(topo, d0, d1)
+    hq = heavy_quartets(topo, d0, d1, int(deriv))
     _native.call("ccsd_b200_eri_s2kl_cart", int(deriv), _native.ptr(atm), _native.ptr(topo.bas_dev),
                  _native.ptr(env), topo.dc_nbas, _native.ptr(topo.ao_loc_dev), d0, d1, naoc, topo.lmax,
                  _native.ptr(hq), int(hq.shape[0]), _native.ptr(cart), st)

@@ -40,7 +40,8 @@ const char *ccsd_b200_last_error(void);
  * entries); nao = ao_loc[nbas]; lmax = max l over the shells.
  * heavy_quartets (int32 x 4, n_heavy entries) must list exactly the block's
  * quartets (i in [ish0, ish1), any j, k >= l) whose Cartesian block has more
- * than 1000 functions: those run on the CTA-cooperative kernel (on a
+ * than 1000 (deriv = 0) or 500 (deriv = 1) functions: those run on the
+ * CTA-cooperative kernel (on a
  * library-owned stream fork/joined with `stream` by events), all others on
  * the warp-per-quartet kernel.
  * Replaces fill_int2e_kernel / fill_int2e_ip1_kernel and the per-i-shell

@@ -32,7 +32,7 @@ def _cart_block(mol, b0, b1, deriv):
     naoc = topo.nao_cart
     ncomp = 3 if deriv else 1
     cart = torch.empty((ncomp, nfc, naoc, naoc * (naoc + 1) // 2), dtype=torch.float64, device=dev)
-    hq = heavy_quartets(topo, d0, d1)
+    hq = heavy_quartets(topo, d0, d1, deriv)
     _native.call("ccsd_b200_eri_s2kl_cart", deriv, _native.ptr(atm), _native.ptr(topo.bas_dev), _native.ptr(env),
                  topo.dc_nbas, _native.ptr(topo.ao_loc_dev), d0, d1, naoc, topo.lmax, _native.ptr(hq),
                  int(hq.shape[0]), _native.ptr(cart), _native.stream())
