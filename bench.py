@@ -47,10 +47,10 @@ import torch
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# DRAM bytes per ip1 quartet of the warp kernel: (1.862656 MB read + 0.073728 MB
-# written) / 8192 quartets, from an ncu capture of this kernel on an
-# 8192-quartet sample of the benchmark set
-ERI_DRAM_BYTES_PER_QUARTET = (1.862656e6 + 0.073728e6) / 8192
+# DRAM bytes per ip1 quartet of one step (warp + CTA kernels): dram__bytes
+# rate x duration from an ncu capture of both kernels on an 8192-quartet
+# sample of the benchmark set, (1.687 MB + 0.900 MB) / 8192 quartets
+ERI_DRAM_BYTES_PER_QUARTET = (1.687e6 + 0.900e6) / 8192
 METRIC = "ERI shell quartets/s (FP64 int2e_ip1, 4096 synthetic shells, Schwarz 1e-12); ERI % FP64 peak"
 NSHELL = 4096
 
@@ -684,9 +684,9 @@ def main():
                    "parallelism": "dp%d" % ws if ws > 1 else "single"},
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak, "traffic": ERI_DRAM_BYTES_PER_QUARTET * nq,
-                     "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of the "
-                                       "ip1 warp kernel on an 8192-quartet sample of this set, scaled per quartet "
-                                       "(shell data is L2-resident; DRAM traffic grows with the quartet count)",
+                     "traffic_source": "DRAM bytes of one ncu capture of the ip1 warp and CTA kernels on an "
+                                       "8192-quartet sample of this set, scaled per quartet (shell data is "
+                                       "L2-resident; DRAM traffic grows with the quartet count)",
                      "peak_source": "FP64 FMA probe measured in this run (driver peaks file has no FP64 figure)",
                      "flops": "reference-algorithm FP64 op count of the sampled quartets"},
         "int2e_quartets_per_s": tot_q / (int2e_ms * 1e-3),
