@@ -206,13 +206,19 @@ LOW_INTENSITY_MAX_K = 1024
 SMALL_FLOPS = 5e7
 
 
+# solvers whose largest contraction (the 2 o^2 v^4 ladder) is below this run
+# in FP64: measured on ethanol/cc-pVDZ (4e9 flops: split precision 0.95x of
+# FP64) and (H2O)3 (5e9: equal); (H2O)6 (3e11) gains 1.35x
+MIXED_MIN_LADDER_FLOPS = 1e10
+
+
 def effective_mode(mode, nocc, nvir):
-    """The mode an iterative solver should run in: split precision gains
-    nothing when even its largest contraction (the o^2 v^4 ladder) is below
-    SMALL_FLOPS, since every contraction then takes the FP64 route anyway; the
-    solver runs in FP64 directly and skips the split-precision phase and the
-    FP64 polish after it."""
-    if mode != "fp64" and 2.0 * nocc * nocc * float(nvir) ** 4 < SMALL_FLOPS:
+    """The mode an iterative solver should run in.  Split precision gains
+    nothing while the largest contraction is small: the packs and launches
+    cost as much as the tensor cores save, and below SMALL_FLOPS every
+    contraction takes the FP64 route anyway.  Such solves run in FP64
+    directly (no split-precision phase, no FP64 polish)."""
+    if mode != "fp64" and 2.0 * nocc * nocc * float(nvir) ** 4 < max(SMALL_FLOPS, MIXED_MIN_LADDER_FLOPS):
         return "fp64"
     return mode
 

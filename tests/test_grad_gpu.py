@@ -19,6 +19,7 @@ def _tensor_cores_at_small_sizes(monkeypatch):
     launch-bound FP64 route; keep the split-precision modes on the tensor cores."""
     import ccsd_gpu_b200.contract as Cn
     monkeypatch.setattr(Cn, "SMALL_FLOPS", 0.0)
+    monkeypatch.setattr(Cn, "MIXED_MIN_LADDER_FLOPS", 0.0)
 
 H2O = "O 0 0 0; H 0 -0.757 0.587; H 0.05 0.757 0.587"
 
