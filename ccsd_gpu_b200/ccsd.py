@@ -16,7 +16,9 @@ import torch
 
 from . import _native
 from .contract import check_status, contract, effective_mode
-from .graphs import StepGraph
+from .graphs import StepGraph, solve_step
+
+_T_CONSTS = ("fock", "mo_energy", "ovov", "ovvv", "ovoo", "ovvo", "oovv", "oooo", "vvvv")
 from .gpu_ccsd_lambda import DIIS, DeviceEris, amplitude_norm_sq, solve_lambda_gpu
 
 
@@ -165,6 +167,9 @@ class CCSD:
         # as it saves over the 12-20 iterations of one gradient (measured on
         # H2O and (H2O)6, cc-pVDZ)
         self.use_graphs = False
+        # FP64 iteration bodies are captured once per (shape, level shift) and
+        # replayed by every later solve of the same shape (integrals copied in)
+        self.use_graph_cache = True
         self.verbose = 0
         self.t1 = self.t2 = self.l1 = self.l2 = None
         self.converged = self.converged_lambda = False
@@ -227,6 +232,11 @@ class CCSD:
 
     def _step(self, eris, mode):
         ls = self.level_shift
+        if mode == "fp64" and self.use_graph_cache and not self.use_graphs:
+            consts = {k: getattr(eris, k) for k in _T_CONSTS}
+            nocc = eris.ovoo.shape[0]
+            key = ("T", nocc, eris.fock.shape[0] - nocc, float(ls))
+            return solve_step(key, lambda c, a, b: update_amps_gpu(a, b, SimpleNamespace(**c), "fp64", ls), consts)
         return StepGraph(lambda a, b: update_amps_gpu(a, b, eris, mode, ls), enabled=self.use_graphs)
 
     @property

@@ -25,7 +25,7 @@ import torch
 
 from . import _native
 from .contract import check_status, contract, effective_mode, mark_constant
-from .graphs import StepGraph
+from .graphs import StepGraph, solve_step
 
 DEFAULT_MODE = "tf32x3"
 
@@ -272,6 +272,9 @@ class DIIS:
         return torch.mv(self.xbuf[:n].T, c)
 
 
+_L_ERIS = ("fock", "mo_energy", "oooo", "ovoo", "ovvo", "oovv", "ovov", "ovvv", "vvvv")
+_L_IMDS = ("w1", "w2", "w3", "w4", "woooo", "wvooo", "wVOov", "wvOOv", "wvvov")
+
 MIXED_FLOOR = 1e-6     # update norm below which split-precision iterations stop helping
 
 
@@ -313,7 +316,21 @@ def kernel_gpu(mycc, eris=None, t1=None, t2=None, l1=None, l2=None, max_cycle=No
     history = []
     graphs = getattr(mycc, "use_graphs", False)
 
+    ls = float(getattr(mycc, "level_shift", 0.0))
+
     def make_step(im, md):
+        if md == "fp64" and getattr(mycc, "use_graph_cache", True) and not graphs:
+            consts = {"e_" + k: getattr(eris, k) for k in _L_ERIS}
+            consts.update({"i_" + k: getattr(im, k) for k in _L_IMDS})
+            consts.update(t1=t1g, t2=t2g)
+            key = ("L", t1g.shape[0], t1g.shape[1], ls)
+            stub = SimpleNamespace(level_shift=ls)
+
+            def body(c, a, b):
+                er = SimpleNamespace(**{k: c["e_" + k] for k in _L_ERIS})
+                imd = SimpleNamespace(mode="fp64", **{k: c["i_" + k] for k in _L_IMDS})
+                return update_lambda_gpu(stub, c["t1"], c["t2"], a, b, er, imd, mode="fp64")
+            return solve_step(key, body, consts)
         return StepGraph(lambda a, b: update_lambda_gpu(mycc, t1g, t2g, a, b, eris, im, mode=md), enabled=graphs)
 
     step = make_step(imds, cur_mode)

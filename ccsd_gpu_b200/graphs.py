@@ -48,3 +48,74 @@ class StepGraph:
             self.enabled = False
             return
         self.graph = g
+
+
+class _SolveGraph:
+    def __init__(self, fn, consts, inputs):
+        self.fn = fn
+        self.consts = {k: v.detach().clone() for k, v in consts.items()}
+        self.static_in = [x.detach().clone() for x in inputs]
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            fn(self.consts, *self.static_in)
+        torch.cuda.current_stream().wait_stream(side)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self.static_out = tuple(fn(self.consts, *self.static_in))
+        self.graph = g
+
+    def load(self, consts):
+        for k, v in consts.items():
+            self.consts[k].copy_(v)
+
+    def __call__(self, *inputs):
+        for d, x in zip(self.static_in, inputs):
+            d.copy_(x)
+        self.graph.replay()
+        return tuple(o.clone() for o in self.static_out)
+
+
+_SOLVE_GRAPHS = {}
+_SOLVE_GRAPHS_MAX = 8
+
+
+def solve_step(key, fn, consts, enabled=True):
+    """A replayable iteration body shared by every solve of the same shape.
+
+    ``fn(consts, *inputs)`` is pure device work on the tensors of the dict
+    ``consts`` (integrals, intermediates: fixed within one solve) and on the
+    per-iteration ``inputs``.  The graph for ``key`` is captured once (the
+    first call runs eagerly); later solves copy their own ``consts`` into the
+    captured tensors and replay.  Only for FP64 bodies: a split-precision body
+    would replay tensor-core packs of operands cached from the capturing solve.
+    """
+    if not (enabled and torch.cuda.is_available()):
+        return lambda *inputs: fn(consts, *inputs)
+    key = (torch.cuda.current_device(),) + tuple(key)
+    entry = _SOLVE_GRAPHS.get(key)
+    state = {"entry": entry, "first": entry is None}
+    if entry is not None:
+        entry.load(consts)
+
+    def step(*inputs):
+        if state["entry"] is None:
+            out = fn(consts, *inputs)
+            try:
+                e = _SolveGraph(fn, consts, inputs)
+            except RuntimeError:                 # not capturable here: stay eager
+                state["entry"] = False
+                return out
+            if len(_SOLVE_GRAPHS) >= _SOLVE_GRAPHS_MAX:
+                _SOLVE_GRAPHS.pop(next(iter(_SOLVE_GRAPHS)))
+            _SOLVE_GRAPHS[key] = e
+            state["entry"] = e
+            return out
+        if state["entry"] is False:
+            return fn(consts, *inputs)
+        return state["entry"](*inputs)
+    return step
+
+
+def clear_solve_graphs():
+    _SOLVE_GRAPHS.clear()

@@ -185,3 +185,27 @@ def test_frozen_core_gradient_matches_finite_differences():
     assert np.abs(grads["fp64"] - fd).max() < 1e-6, np.abs(grads["fp64"] - fd).max()
     assert np.abs(grads["tf32x3"] - grads["fp64"]).max() < 1e-6
     assert np.abs(grads["fp64"].sum(0)).max() < 1e-8
+
+
+def test_cached_fp64_solve_graphs_match_eager_across_geometries():
+    """FP64 T/Lambda bodies replayed from the cross-solve graph cache: a second
+    geometry (new integrals copied into the captured tensors) gives the eager
+    energy and gradient."""
+    from ccsd_gpu_b200.ccsd import CCSD
+    from ccsd_gpu_b200.graphs import clear_solve_graphs
+    from ccsd_gpu_b200.gto import M
+    from ccsd_gpu_b200.scf import RHF
+    clear_solve_graphs()
+    geoms = [H2O, "O 0 0 0.02; H 0 -0.74 0.60; H 0.03 0.77 0.57"]
+    for atom in geoms:
+        mf = RHF(M(atom=atom, basis="cc-pvdz")).run()
+        out = {}
+        for cached in (True, False):
+            cc = CCSD(mf, precision="fp64")
+            cc.use_graph_cache = cached
+            cc.kernel()
+            cc.conv_tol_normt = 1e-9
+            cc.solve_lambda()
+            out[cached] = (cc.e_tot, cc.nuc_grad_method().kernel())
+        assert abs(out[True][0] - out[False][0]) < 1e-10
+        assert np.abs(out[True][1] - out[False][1]).max() < 1e-9
