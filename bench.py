@@ -694,7 +694,7 @@ def main():
         "timed_region_ms": region_ms,
         "e2e": {"value": tot_q / (e2e_ms * 1e-3), "unit": "quartets/s", "h2d_bytes_per_step": nq * 16,
                 "d2h_bytes_per_step": nq * 3 * 2 * 8},
-        "gpu_launches": args.steps,
+        "gpu_launches": 2 * args.steps,     # per step: the warp-per-quartet and the CTA (heavy) kernel
         "clocks": clk.summary(),
         "cpu_baseline": cpu,
         "parity_vs_reference_max": parity,
