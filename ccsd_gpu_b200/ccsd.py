@@ -16,10 +16,10 @@ import torch
 
 from . import _native
 from .contract import check_status, contract, effective_mode
-from .graphs import StepGraph, solve_step
+from .graphs import StepGraph, graph_cache_ok, solve_step
 
 _T_CONSTS = ("fock", "mo_energy", "ovov", "ovvv", "ovoo", "ovvo", "oovv", "oooo", "vvvv")
-from .gpu_ccsd_lambda import DIIS, DeviceEris, amplitude_norm_sq, solve_lambda_gpu
+from .gpu_ccsd_lambda import DIIS, DeviceEris, amplitude_norm_sq, host_copy, remember_device, solve_lambda_gpu
 
 
 def ao2mo_gpu(mf, mo_coeff=None, frozen=0):
@@ -226,17 +226,19 @@ class CCSD:
             e_old = e
         check_status()
         self.e_corr = e
-        self._t1g, self._t2g = t1, t2
-        self.t1, self.t2 = t1.cpu().numpy(), t2.cpu().numpy()
+        self.t1, self.t2 = host_copy(t1), host_copy(t2)
+        remember_device(self, "t1", self.t1, t1)
+        remember_device(self, "t2", self.t2, t2)
         return self.e_corr, self.t1, self.t2
 
     def _step(self, eris, mode):
         ls = self.level_shift
-        if mode == "fp64" and self.use_graph_cache and not self.use_graphs:
+        nocc = eris.ovoo.shape[0]
+        nvir = eris.fock.shape[0] - nocc
+        if self.use_graph_cache and not self.use_graphs and graph_cache_ok(mode, nocc, nvir):
             consts = {k: getattr(eris, k) for k in _T_CONSTS}
-            nocc = eris.ovoo.shape[0]
-            key = ("T", nocc, eris.fock.shape[0] - nocc, float(ls))
-            return solve_step(key, lambda c, a, b: update_amps_gpu(a, b, SimpleNamespace(**c), "fp64", ls), consts)
+            key = ("T", nocc, nvir, float(ls), mode)
+            return solve_step(key, lambda c, a, b: update_amps_gpu(a, b, SimpleNamespace(**c), mode, ls), consts)
         return StepGraph(lambda a, b: update_amps_gpu(a, b, eris, mode, ls), enabled=self.use_graphs)
 
     @property

@@ -112,6 +112,20 @@ def _dev_offsets(key, make, dev):
 _const = {}                  # storage data_ptr -> weakref to the registered tensor
 _pack_cache = {}             # key -> (hi, lo)
 _PACK_CACHE_BYTES = 64 << 30
+# switched off while a CUDA graph that is replayed with new operand values is
+# captured: the graph must contain the packs, not read packs cached earlier
+_PACK_CACHE_ON = [True]
+
+
+class pack_cache_disabled:
+    """Context manager: no packed-operand cache lookups or inserts inside."""
+
+    def __enter__(self):
+        self.prev = _PACK_CACHE_ON[0]
+        _PACK_CACHE_ON[0] = False
+
+    def __exit__(self, *exc):
+        _PACK_CACHE_ON[0] = self.prev
 
 
 def mark_constant(*tensors):
@@ -149,7 +163,7 @@ def _cache_key(terms, sub, rows_idx, k_idx, shape_map, kind, rows_pad, k_pad):
 
 
 def _pack(terms, sub, rows_idx, k_idx, shape_map, kind, rows_pad, k_pad, dev, stream):
-    key = _cache_key(terms, sub, rows_idx, k_idx, shape_map, kind, rows_pad, k_pad)
+    key = _cache_key(terms, sub, rows_idx, k_idx, shape_map, kind, rows_pad, k_pad) if _PACK_CACHE_ON[0] else None
     if key is not None and key in _pack_cache:
         return _pack_cache[key]
     hi, lo = _pack_new(terms, sub, rows_idx, k_idx, shape_map, kind, rows_pad, k_pad, dev, stream)

@@ -27,6 +27,7 @@ import torch
 
 from . import _native
 from .contract import contract
+from .gpu_ccsd_lambda import device_amp
 from .cuda.ip1_contract import contract_int2e_ip1
 from .int1e import intor1e
 
@@ -311,6 +312,8 @@ class Gradients:
             if cc.l1 is None:
                 cc.solve_lambda()
             l1, l2 = cc.l1, cc.l2
+        t1, t2 = device_amp(cc, "t1", t1), device_amp(cc, "t2", t2)
+        l1, l2 = device_amp(cc, "l1", l1), device_amp(cc, "l2", l2)
         self.de = grad_elec_gpu(cc, t1, t2, l1, l2) + cc.mol.grad_nuc()
         return self.de
 

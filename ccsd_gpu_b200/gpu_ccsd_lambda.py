@@ -25,7 +25,7 @@ import torch
 
 from . import _native
 from .contract import check_status, contract, effective_mode, mark_constant
-from .graphs import StepGraph, solve_step
+from .graphs import StepGraph, graph_cache_ok, solve_step
 
 DEFAULT_MODE = "tf32x3"
 
@@ -60,6 +60,32 @@ class DeviceEris:
     @classmethod
     def wrap(cls, eris):
         return eris if isinstance(eris, cls) else cls(eris)
+
+
+def host_copy(x):
+    """Read-only numpy copy of the device tensor ``x``, read into pinned host
+    memory (torch's caching host allocator reuses the block once the array is
+    dropped; a pageable read of a 100 MB amplitude runs at ~4 GB/s)."""
+    h = torch.empty(x.shape, dtype=x.dtype, pin_memory=True)
+    h.copy_(x)
+    a = h.numpy()
+    a.setflags(write=False)
+    return a
+
+
+def remember_device(mycc, name, host, dev):
+    """Record that the host array ``mycc.<name>`` (``host``) has the device
+    copy ``dev``, so later steps of the chain skip the round trip.  ``host``
+    is read-only (``host_copy``), so the pair cannot drift apart."""
+    d = mycc.__dict__.setdefault("_dev_amps", {})
+    d[name] = (host, dev)
+
+
+def device_amp(mycc, name, value):
+    """The device copy of ``value`` if it is the array this package produced
+    for ``mycc.<name>`` (identity check), else ``value`` itself."""
+    d = getattr(mycc, "_dev_amps", {}).get(name)
+    return d[1] if d is not None and d[0] is value else value
 
 
 class _Ctx:
@@ -292,8 +318,8 @@ def kernel_gpu(mycc, eris=None, t1=None, t2=None, l1=None, l2=None, max_cycle=No
     if eris is None:
         eris = mycc.ao2mo()
     eris = DeviceEris.wrap(eris)
-    t1 = mycc.t1 if t1 is None else t1
-    t2 = mycc.t2 if t2 is None else t2
+    t1 = device_amp(mycc, "t1", mycc.t1 if t1 is None else t1)
+    t2 = device_amp(mycc, "t2", mycc.t2 if t2 is None else t2)
     l1 = t1 if l1 is None else l1
     l2 = t2 if l2 is None else l2
     max_cycle = getattr(mycc, "max_cycle", 50) if max_cycle is None else max_cycle
@@ -319,17 +345,17 @@ def kernel_gpu(mycc, eris=None, t1=None, t2=None, l1=None, l2=None, max_cycle=No
     ls = float(getattr(mycc, "level_shift", 0.0))
 
     def make_step(im, md):
-        if md == "fp64" and getattr(mycc, "use_graph_cache", True) and not graphs:
+        if getattr(mycc, "use_graph_cache", True) and not graphs and graph_cache_ok(md, *t1g.shape):
             consts = {"e_" + k: getattr(eris, k) for k in _L_ERIS}
             consts.update({"i_" + k: getattr(im, k) for k in _L_IMDS})
             consts.update(t1=t1g, t2=t2g)
-            key = ("L", t1g.shape[0], t1g.shape[1], ls)
+            key = ("L", t1g.shape[0], t1g.shape[1], ls, md)
             stub = SimpleNamespace(level_shift=ls)
 
             def body(c, a, b):
                 er = SimpleNamespace(**{k: c["e_" + k] for k in _L_ERIS})
-                imd = SimpleNamespace(mode="fp64", **{k: c["i_" + k] for k in _L_IMDS})
-                return update_lambda_gpu(stub, c["t1"], c["t2"], a, b, er, imd, mode="fp64")
+                imd = SimpleNamespace(mode=md, **{k: c["i_" + k] for k in _L_IMDS})
+                return update_lambda_gpu(stub, c["t1"], c["t2"], a, b, er, imd, mode=md)
             return solve_step(key, body, consts)
         return StepGraph(lambda a, b: update_lambda_gpu(mycc, t1g, t2g, a, b, eris, im, mode=md), enabled=graphs)
 
@@ -355,7 +381,8 @@ def kernel_gpu(mycc, eris=None, t1=None, t2=None, l1=None, l2=None, max_cycle=No
             break
     check_status()
     mycc._lambda_history = history
-    return conv, l1g.cpu().numpy(), l2g.cpu().numpy()
+    mycc._last_lambda_dev = (l1g, l2g)
+    return conv, host_copy(l1g), host_copy(l2g)
 
 
 def solve_lambda_gpu(mycc, t1=None, t2=None, l1=None, l2=None, eris=None, use_cpu_vvvv=True,
@@ -370,5 +397,8 @@ def solve_lambda_gpu(mycc, t1=None, t2=None, l1=None, l2=None, eris=None, use_cp
     mycc.converged_lambda = conv
     mycc.l1 = l1o
     mycc.l2 = l2o
+    l1g, l2g = mycc.__dict__.pop("_last_lambda_dev")
+    remember_device(mycc, "l1", l1o, l1g)
+    remember_device(mycc, "l2", l2o, l2g)
     mycc._lambda_solver_mode = "gpu-" + _mode_of(mycc, mode)
     return mycc.l1, mycc.l2

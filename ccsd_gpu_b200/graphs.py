@@ -52,17 +52,21 @@ class StepGraph:
 
 class _SolveGraph:
     def __init__(self, fn, consts, inputs):
+        from .contract import mark_constant, pack_cache_disabled
         self.fn = fn
         self.consts = {k: v.detach().clone() for k, v in consts.items()}
+        # constants as in the eager solve, so contractions take the same routes
+        mark_constant(*self.consts.values())
         self.static_in = [x.detach().clone() for x in inputs]
-        side = torch.cuda.Stream()
-        side.wait_stream(torch.cuda.current_stream())
-        with torch.cuda.stream(side):
-            fn(self.consts, *self.static_in)
-        torch.cuda.current_stream().wait_stream(side)
-        g = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(g):
-            self.static_out = tuple(fn(self.consts, *self.static_in))
+        with pack_cache_disabled():         # packs of the constants become graph nodes
+            side = torch.cuda.Stream()
+            side.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(side):
+                fn(self.consts, *self.static_in)
+            torch.cuda.current_stream().wait_stream(side)
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                self.static_out = tuple(fn(self.consts, *self.static_in))
         self.graph = g
 
     def load(self, consts):
@@ -77,7 +81,15 @@ class _SolveGraph:
 
 
 _SOLVE_GRAPHS = {}
-_SOLVE_GRAPHS_MAX = 8
+_SOLVE_GRAPHS_MAX = 32
+# split-precision bodies are cached only while their ladder (2 o^2 v^4 flops)
+# is below this: beyond it the per-replay re-pack of the integrals costs more
+# than the host overhead a graph saves
+GRAPH_MAX_LADDER_FLOPS = 1e12
+
+
+def graph_cache_ok(mode, nocc, nvir):
+    return mode == "fp64" or 2.0 * nocc * nocc * float(nvir) ** 4 < GRAPH_MAX_LADDER_FLOPS
 
 
 def solve_step(key, fn, consts, enabled=True):
@@ -87,8 +99,10 @@ def solve_step(key, fn, consts, enabled=True):
     ``consts`` (integrals, intermediates: fixed within one solve) and on the
     per-iteration ``inputs``.  The graph for ``key`` is captured once (the
     first call runs eagerly); later solves copy their own ``consts`` into the
-    captured tensors and replay.  Only for FP64 bodies: a split-precision body
-    would replay tensor-core packs of operands cached from the capturing solve.
+    captured tensors and replay.  The packed-operand cache is off during the
+    capture, so a split-precision body re-packs its constant operands inside
+    the graph on every replay (from the captured tensors, i.e. the current
+    solve's values).
     """
     if not (enabled and torch.cuda.is_available()):
         return lambda *inputs: fn(consts, *inputs)

@@ -209,3 +209,44 @@ def test_cached_fp64_solve_graphs_match_eager_across_geometries():
             out[cached] = (cc.e_tot, cc.nuc_grad_method().kernel())
         assert abs(out[True][0] - out[False][0]) < 1e-10
         assert np.abs(out[True][1] - out[False][1]).max() < 1e-9
+
+
+def test_cached_split_precision_solve_graphs_match_eager_across_geometries():
+    """The same for tf32x3 bodies: packs of the integrals are graph nodes, so a
+    second geometry replays with its own integrals."""
+    from ccsd_gpu_b200.ccsd import CCSD
+    from ccsd_gpu_b200.graphs import clear_solve_graphs
+    from ccsd_gpu_b200.gto import M
+    from ccsd_gpu_b200.scf import RHF
+    clear_solve_graphs()
+    for atom in (H2O, "O 0 0 0.02; H 0 -0.74 0.60; H 0.03 0.77 0.57"):
+        mf = RHF(M(atom=atom, basis="cc-pvdz")).run()
+        out = {}
+        for cached in (True, False):
+            cc = CCSD(mf, precision="tf32x3")
+            cc.use_graph_cache = cached
+            cc.t_polish = cc.lambda_polish = False
+            cc.kernel()
+            cc.conv_tol_normt = 1e-9
+            cc.solve_lambda()
+            out[cached] = (cc.e_tot, cc.nuc_grad_method().kernel())
+        assert abs(out[True][0] - out[False][0]) < 1e-9
+        assert np.abs(out[True][1] - out[False][1]).max() < 1e-8
+
+
+def test_device_amplitude_hand_off_matches_host_arrays(h2o_oracle):
+    """The solves keep device copies of t1/t2/l1/l2 next to their (read-only)
+    host arrays; the gradient from that hand-off equals the one from fresh
+    host copies, which take the upload path."""
+    from ccsd_gpu_b200.ccsd import CCSD
+    from ccsd_gpu_b200.scf import RHF
+    cc = CCSD(RHF(h2o_oracle["mol"]).run(), precision="fp64")
+    cc.kernel()
+    cc.conv_tol_normt = 1e-9
+    cc.solve_lambda()
+    for a in (cc.t1, cc.t2, cc.l1, cc.l2):
+        assert not a.flags.writeable
+    g_dev = cc.nuc_grad_method().kernel()
+    g_host = cc.nuc_grad_method().kernel(*(np.array(a) for a in (cc.t1, cc.t2, cc.l1, cc.l2)))
+    assert np.abs(g_dev - g_host).max() < 1e-12
+    assert np.abs(g_dev - h2o_oracle["grad"]).max() < 1e-7
