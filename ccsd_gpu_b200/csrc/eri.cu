@@ -81,6 +81,85 @@ __device__ __forceinline__ Shell load_shell(const int *__restrict__ atm, const i
     return s;
 }
 
+// Primitive-pair screen.  A pair of Gaussians with exponents a, b on centres
+// A, B carries exp(-ab/(a+b) |AB|^2) in every integral it enters; the pair is
+// dropped when ab/(a+b) |AB|^2 > kPairCut + (la + lb) ln(1 + |AB|), the second
+// term allowing for the polynomial factors (P-A)^i (P-B)^j of the pair's
+// Cartesian functions (|P-A|, |P-B| <= |AB|).  e^-50 ~ 2e-22 relative to an
+// O(1) normalised primitive product: far below FP64 resolution of any block.
+// The kept pairs of one shell pair are a 128-bit mask in registers (bit
+// ia * nb + ib), built with warp ballots; pairs beyond 128 are not screened.
+static constexpr double kPairCut = 50.0;
+
+struct PairMask {
+    unsigned w[4];
+    int n;      // kept pairs
+    int nb;     // primitives of the second shell
+    int all;    // more than 128 pairs: every pair kept, index decoded directly
+};
+
+// Every lane of the calling warp must be active (warp ballots).
+__device__ __forceinline__ PairMask pair_mask(const Shell &a, const Shell &b, double r2, int lsum)
+{
+    PairMask m;
+    const int n = a.np * b.np;
+    m.nb = b.np;
+    m.all = n > 128;
+    m.n = m.all ? n : 0;
+    const double cut = kPairCut + lsum * log1p(sqrt(r2));
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        const int t = c * 32 + lane;
+        bool keep = false;
+        if (!m.all && t < n) {
+            const int ia = t / b.np, ib = t - ia * b.np;
+            const double ea = a.exps[ia], eb = b.exps[ib];
+            keep = ea * eb / (ea + eb) * r2 <= cut;
+        }
+        m.w[c] = __ballot_sync(0xffffffffu, keep);
+        if (!m.all) m.n += __popc(m.w[c]);
+    }
+    return m;
+}
+
+// Position of the k-th (0-based) set bit of w; w has more than k set bits.
+__device__ __forceinline__ int nth_set_bit(unsigned w, int k)
+{
+    int pos = 0;
+#pragma unroll
+    for (int half = 16; half > 0; half >>= 1) {
+        const unsigned lo = w & ((1u << half) - 1u);
+        const int c = __popc(lo);
+        if (k >= c) {
+            k -= c;
+            w >>= half;
+            pos += half;
+        } else {
+            w = lo;
+        }
+    }
+    return pos;
+}
+
+// Primitive indices of the k-th kept pair.
+__device__ __forceinline__ void kept_pair(const PairMask &m, int k, int &ia, int &ib)
+{
+    int t = k;
+    if (!m.all) {
+        int c = 0;
+        while (c < 3) {
+            const int pc = __popc(m.w[c]);
+            if (k < pc) break;
+            k -= pc;
+            c++;
+        }
+        t = c * 32 + nth_set_bit(m.w[c], k);
+    }
+    ia = t / m.nb;
+    ib = t - ia * m.nb;
+}
+
 __device__ __forceinline__ double common_fac(int l)
 {
     return l == 0 ? 0.282094791773878143 : (l == 1 ? 0.488602511902919921 : 1.0);
@@ -256,8 +335,6 @@ __device__ void eri_quartet(const int *__restrict__ atm, const int *__restrict__
     const int nf = nfi * nfj * nfk * nfl;
     const int nroots = (li + lj + lk + ll + D) / 2 + 1;
     const int sj = li + 1 + D, sk = sj * (lj + 1), sl = sk * (lk + 1), gsz = sl * (ll + 1);
-    const int npq = si.np * sj_.np * sk_.np * sl_.np;
-    const int nslot = npq * nroots;
     int ns = smem_warp / (3 * gsz + kParStride);
     ns = ns > kMaxSlots ? kMaxSlots : ns;
     double *par = wsm;
@@ -269,6 +346,8 @@ __device__ void eri_quartet(const int *__restrict__ atm, const int *__restrict__
     }
     const double rab2 = AB[0] * AB[0] + AB[1] * AB[1] + AB[2] * AB[2];
     const double rcd2 = CD[0] * CD[0] + CD[1] * CD[1] + CD[2] * CD[2];
+    const PairMask mb = pair_mask(si, sj_, rab2, li + lj + D), mk = pair_mask(sk_, sl_, rcd2, lk + ll);
+    const int nslot = mb.n * mk.n * nroots;
     const double pref0 = 34.986836655249725693 * common_fac(li) * common_fac(lj) * common_fac(lk) *
                          common_fac(ll);   // 2 pi^(5/2) x angular factors of s, p
 
@@ -310,11 +389,9 @@ __device__ void eri_quartet(const int *__restrict__ atm, const int *__restrict__
             // ---- phase A: primitive-quartet data and Rys nodes/weights
             const int pq0 = s0 / nroots, pq1 = (s1 - 1) / nroots + 1;
             for (int pq = pq0 + lane; pq < pq1; pq += 32) {
-                int t = pq;
-                const int lp = t % sl_.np; t /= sl_.np;
-                const int kp = t % sk_.np; t /= sk_.np;
-                const int jp = t % sj_.np;
-                const int ip = t / sj_.np;
+                int ip, jp, kp, lp;
+                kept_pair(mb, pq / mk.n, ip, jp);
+                kept_pair(mk, pq % mk.n, kp, lp);
                 const double ai = si.exps[ip], aj = sj_.exps[jp], ak = sk_.exps[kp], al = sl_.exps[lp];
                 const double aij = ai + aj, akl = ak + al, aijkl = aij + akl;
                 double PA[3], QC[3], PQ[3];
@@ -694,8 +771,6 @@ __device__ void eri_quartet_hc(const int *__restrict__ atm, const int *__restric
     const int li = si.l, lj = sj_.l, lk = sk_.l, ll = sl_.l;      // computed orientation
     const int le = li + lj + D, lf = lk + ll, s2 = (le + 1) * (lf + 1);
     const int nroots = (li + lj + lk + ll + D) / 2 + 1;
-    const int npq = si.np * sj_.np * sk_.np * sl_.np;
-    const int nslot = npq * nroots;
     int ns = cap / (3 * s2 + kParStride);
     ns = ns > kMaxSlots ? kMaxSlots : ns;
     double *par = wsm;
@@ -707,6 +782,8 @@ __device__ void eri_quartet_hc(const int *__restrict__ atm, const int *__restric
     }
     const double rab2 = AB[0] * AB[0] + AB[1] * AB[1] + AB[2] * AB[2];
     const double rcd2 = CD[0] * CD[0] + CD[1] * CD[1] + CD[2] * CD[2];
+    const PairMask mb = pair_mask(si, sj_, rab2, li + lj + D), mk = pair_mask(sk_, sl_, rcd2, lk + ll);
+    const int nslot = mb.n * mk.n * nroots;
     const double pref0 = 34.986836655249725693 * common_fac(li) * common_fac(lj) * common_fac(lk) *
                          common_fac(ll);
 
@@ -739,11 +816,9 @@ __device__ void eri_quartet_hc(const int *__restrict__ atm, const int *__restric
         // ---- phase A: primitive-quartet data and Rys nodes/weights (as in eri_quartet)
         const int pq0 = s0 / nroots, pq1 = (s1 - 1) / nroots + 1;
         for (int pq = pq0 + lane; pq < pq1; pq += NT) {
-            int t = pq;
-            const int lp = t % sl_.np; t /= sl_.np;
-            const int kp = t % sk_.np; t /= sk_.np;
-            const int jp = t % sj_.np;
-            const int ip = t / sj_.np;
+            int ip, jp, kp, lp;
+            kept_pair(mb, pq / mk.n, ip, jp);
+            kept_pair(mk, pq % mk.n, kp, lp);
             const double ai = si.exps[ip], aj = sj_.exps[jp], ak = sk_.exps[kp], al = sl_.exps[lp];
             const double aij = ai + aj, akl = ak + al, aijkl = aij + akl;
             double PA[3], QC[3], PQ[3];
@@ -1001,7 +1076,6 @@ __device__ void eri_quartet_cta(const int *__restrict__ atm, const int *__restri
     const int ne = nf * NC;
     const int nroots = (li + lj + lk + ll + D) / 2 + 1;
     const int sj = li + 1 + D, sk = sj * (lj + 1), sl = sk * (lk + 1), gsz = sl * (ll + 1);
-    const int nslot = si.np * sj_.np * sk_.np * sl_.np * nroots;
     int ns = smem_doubles / (3 * gsz + kParStride);
     ns = ns > kMaxSlots ? kMaxSlots : ns;
     double *par = sm;
@@ -1013,6 +1087,8 @@ __device__ void eri_quartet_cta(const int *__restrict__ atm, const int *__restri
     }
     const double rab2 = AB[0] * AB[0] + AB[1] * AB[1] + AB[2] * AB[2];
     const double rcd2 = CD[0] * CD[0] + CD[1] * CD[1] + CD[2] * CD[2];
+    const PairMask mb = pair_mask(si, sj_, rab2, li + lj + D), mk = pair_mask(sk_, sl_, rcd2, lk + ll);
+    const int nslot = mb.n * mk.n * nroots;
     const double pref0 = 34.986836655249725693 * common_fac(li) * common_fac(lj) * common_fac(lk) * common_fac(ll);
     double qv[6] = {0, 0, 0, 0, 0, 0};
 
@@ -1047,11 +1123,9 @@ __device__ void eri_quartet_cta(const int *__restrict__ atm, const int *__restri
             __syncthreads();
             const int pq0 = s0 / nroots, pq1 = (s1 - 1) / nroots + 1;
             for (int pq = pq0 + tid; pq < pq1; pq += kHeavyThreads) {
-                int t = pq;
-                const int lp = t % sl_.np; t /= sl_.np;
-                const int kp = t % sk_.np; t /= sk_.np;
-                const int jp = t % sj_.np;
-                const int ip = t / sj_.np;
+                int ip, jp, kp, lp;
+                kept_pair(mb, pq / mk.n, ip, jp);
+                kept_pair(mk, pq % mk.n, kp, lp);
                 const double ai = si.exps[ip], aj = sj_.exps[jp], ak = sk_.exps[kp], al = sl_.exps[lp];
                 const double aij = ai + aj, akl = ak + al, aijkl = aij + akl;
                 double PA[3], QC[3], PQ[3];

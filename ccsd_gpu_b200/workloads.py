@@ -131,14 +131,46 @@ def reference_flops(li, lj, lk, ll, npi, npj, npk, npl, deriv):
     return per_prim * npi * npj * npk * npl
 
 
-def quartet_flops(shells, q, deriv):
+PAIR_CUT = 50.0     # primitive-pair screen of the ERI kernels (csrc/eri.cu kPairCut)
+
+
+def kept_pairs(shells, i, j, extra_l=0, chunk=1 << 16):
+    """Primitive pairs of the shell pairs (i[n], j[n]) that the ERI kernels
+    keep: ab/(a+b) |AB|^2 <= PAIR_CUT + (li + lj + extra_l) ln(1 + |AB|)."""
+    b, env, atm = shells._bas, shells._env, shells._atm
+    i, j = np.asarray(i), np.asarray(j)
+    mp = int(b[:, 2].max())
+    E = np.full((len(b), mp), np.nan)
+    for s in range(len(b)):
+        E[s, :b[s, 2]] = env[b[s, 5]:b[s, 5] + b[s, 2]]
+    R = np.stack([env[atm[b[s, 0], 1]:atm[b[s, 0], 1] + 3] for s in range(len(b))])
+    out = np.empty(len(i), dtype=np.int64)
+    for c0 in range(0, len(i), chunk):
+        ii, jj = i[c0:c0 + chunk], j[c0:c0 + chunk]
+        r2 = ((R[ii] - R[jj]) ** 2).sum(1)
+        cut = PAIR_CUT + (b[ii, 1] + b[jj, 1] + extra_l) * np.log1p(np.sqrt(r2))
+        ea, eb = E[ii][:, :, None], E[jj][:, None, :]
+        with np.errstate(invalid="ignore"):
+            th = ea * eb / (ea + eb) * r2[:, None, None]
+            out[c0:c0 + chunk] = (th <= cut[:, None, None]).sum((1, 2))   # NaN (padding) compares False
+    return out
+
+
+def quartet_flops(shells, q, deriv, screened=True):
+    """FP64 op count of the quartets q under the reference algorithm, over the
+    primitive quartets that pass the kernels' pair screen (all of them with
+    ``screened=False``)."""
     b = shells._bas
     l = b[:, 1][q]
-    npr = b[:, 2][q]
+    if screened:
+        w = kept_pairs(shells, q[:, 0], q[:, 1], deriv) * kept_pairs(shells, q[:, 2], q[:, 3])
+    else:
+        w = b[:, 2][q].prod(1)
     total = 0
-    keys, counts = np.unique(np.concatenate([l, npr], 1), axis=0, return_counts=True)
-    for key, c in zip(keys, counts):
-        total += int(c) * reference_flops(*[int(v) for v in key], deriv)
+    keys, inv = np.unique(l, axis=0, return_inverse=True)
+    wsum = np.bincount(inv.reshape(-1), weights=w.astype(np.float64), minlength=len(keys))
+    for key, c in zip(keys, wsum):
+        total += int(round(c)) * reference_flops(*[int(v) for v in key], 1, 1, 1, 1, deriv)
     return total
 
 

@@ -92,6 +92,20 @@ def test_bench_workload_sample_matches_oracle():
         assert checksums_close(got, oracle_eri.quartet_checksums(sh, q, deriv), nf), deriv
 
 
+def test_water_dimer_blocks_with_screened_primitive_pairs_match_oracle():
+    """Intermolecular shell pairs of a water dimer (cc-pVDZ, O 1s exponents up
+    to 1.2e4) lose most primitive pairs to the kernels' pair screen; the blocks
+    still equal the unscreened oracle to rtol 1e-10."""
+    from ccsd_gpu_b200 import compute_int2e_gpu, compute_int2e_ip1_gpu, workloads
+    from ccsd_gpu_b200.gto import M
+    cl = workloads.water_clusters(64, seed=0)
+    s, x = next(c for c in cl if len(c[0]) == 6)
+    mol = M(atom=workloads.atom_string(s, x), basis="cc-pvdz")
+    for b0, b1 in [(0, 2), (11, 13), (mol.nbas - 3, mol.nbas)]:
+        assert block_close(_np(compute_int2e_gpu(mol, b0, b1)), oracle_eri.s2kl(mol, b0, b1, 0)), (b0, b1)
+        assert block_close(_np(compute_int2e_ip1_gpu(mol, b0, b1)), oracle_eri.s2kl(mol, b0, b1, 1)), (b0, b1)
+
+
 def test_invalid_arguments_are_rejected_on_host():
     from ccsd_gpu_b200 import _native
     from ccsd_gpu_b200.gto import M
