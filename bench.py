@@ -49,8 +49,8 @@ sys.path.insert(0, ROOT)
 
 # DRAM bytes per ip1 quartet of one step (warp + CTA kernels): dram__bytes
 # rate x duration from an ncu capture of both kernels on an 8192-quartet
-# sample of the benchmark set, (1.687 MB + 0.900 MB) / 8192 quartets
-ERI_DRAM_BYTES_PER_QUARTET = (1.687e6 + 0.900e6) / 8192
+# sample of the benchmark set, (1.742 MB + 0.926 MB) / 8192 quartets
+ERI_DRAM_BYTES_PER_QUARTET = (1.742e6 + 0.926e6) / 8192
 METRIC = "ERI shell quartets/s (FP64 int2e_ip1, 4096 synthetic shells, Schwarz 1e-12); ERI % FP64 peak"
 NSHELL = 4096
 
