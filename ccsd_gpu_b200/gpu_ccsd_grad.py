@@ -240,12 +240,17 @@ def grad_elec_gpu(mycc, t1, t2, l1, l2, atmlst=None, verbose=None):
     # relaxed density (ref: ccsd_gpu/gpu_ccsd_grad.py:416-500, de_k and vhf1)
     # in one density, symmetrised in k <-> l, contracted with int2e_ip1 that
     # is recomputed shell quartet by shell quartet and never stored.
+    # dm2 is already symmetric in k <-> l and so are P (x) dm1p and dm1p (x) P
+    # (both densities are symmetric); the exchange products are symmetrised
+    # term by term.  Broadcast in-place updates: no (nao,)*4 temporaries.
     gam = dm2
     del dm2
-    gam += P[:, :, None, None] * dm1p[None, None] + dm1p[:, :, None, None] * P[None, None]
-    gam -= 0.5 * torch.einsum("il,kj->ijkl", P, dm1p)
-    gam -= 0.5 * torch.einsum("jk,il->ijkl", P, dm1p)
-    gam = 0.5 * (gam + gam.permute(0, 1, 3, 2))
+    gam.addcmul_(P[:, :, None, None], dm1p[None, None])                       # P_ij D_kl
+    gam.addcmul_(dm1p[:, :, None, None], P[None, None])                       # D_ij P_kl
+    gam.addcmul_(P[:, None, None, :], dm1p.T[None, :, :, None], value=-0.25)   # P_il D_kj
+    gam.addcmul_(P[:, None, :, None], dm1p.T[None, :, None, :], value=-0.25)   # P_ik D_lj
+    gam.addcmul_(dm1p[:, None, None, :], P[None, :, :, None], value=-0.25)     # D_il P_jk
+    gam.addcmul_(dm1p[:, None, :, None], P[None, :, None, :], value=-0.25)     # D_ik P_jl
     de -= contract_int2e_ip1(mol, gam)
     del gam
     charges = mol.atom_charges()

@@ -93,9 +93,22 @@ class RHF:
         dm = torch.as_tensor(dm, dtype=torch.float64, device=self.eri.device)
         return (torch.einsum("pqrs,rs->pq", self.eri, dm), torch.einsum("prqs,rs->pq", self.eri, dm))
 
+    def _coulomb_exchange(self):
+        """G[pq, rs] = (pq|rs) - 1/2 (pr|qs) as an (n^2, n^2) matrix, built once
+        per geometry: each Fock build is then one matrix-vector product that
+        streams G at HBM bandwidth instead of a strided exchange contraction."""
+        if getattr(self, "_G", None) is None:
+            e = self.eri
+            n = e.shape[0]
+            g = e.clone()
+            g.sub_(e.permute(0, 2, 1, 3), alpha=0.5)
+            self._G = g.view(n * n, n * n)
+        return self._G
+
     def get_veff(self, mol=None, dm=None):
-        J, K = self.get_jk(mol, dm)
-        return J - 0.5 * K
+        dm = torch.as_tensor(dm, dtype=torch.float64, device=self.eri.device)
+        n = dm.shape[0]
+        return (self._coulomb_exchange() @ dm.reshape(n * n)).view(n, n)
 
     def energy_nuc(self):
         return self.mol.energy_nuc()
@@ -118,8 +131,8 @@ class RHF:
         dm = 2 * C[:, :nocc] @ C[:, :nocc].T
         fs, errs = [], []
         e_old = 0.0
+        F = h + self.get_veff(dm=dm)
         for it in range(self.max_cycle):
-            F = h + self.get_veff(dm=dm)
             err = F @ dm @ S - S @ dm @ F
             fs.append(F)
             errs.append(err)
@@ -140,10 +153,9 @@ class RHF:
             Fn = h + self.get_veff(dm=dm_new)
             etot = float(0.5 * (dm_new * (h + Fn)).sum()) + self.energy_nuc()
             done = abs(etot - e_old) < self.conv_tol and float((dm_new - dm).abs().max()) < 1e-8
-            dm, e_old = dm_new, etot
+            dm, e_old, F = dm_new, etot, Fn
             if done:
                 break
-        F = h + self.get_veff(dm=dm)
         e, Cp = torch.linalg.eigh(X.T @ F @ X)
         self.mo_energy_t, self.mo_coeff_t = e, X @ Cp
         self.mo_energy = e.cpu().numpy()
