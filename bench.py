@@ -75,6 +75,7 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--quartets", type=int, default=1 << 18, help="sampled quartets per rank per step")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU-baseline sample budget")
+    ap.add_argument("--no-tune", action="store_true", help="ERI workload: compiled heavy-quartet thresholds")
     args = ap.parse_args()
     dflt = {"eri": (10, 3), "lambda": (3, 3), "gemm": (10, 3), "grad": (5, 3), "autograd": (3, 3),
             "clusters": (1, 1)}[args.workload]     # clusters: one warm-up pass fills the basis caches
@@ -628,6 +629,12 @@ def main():
         barrier()
         return np.array([a.elapsed_time(b) for a, b in evs]), t0.elapsed_time(t1)
 
+    # autotuner (before warm-up, outside every timed region): heavy-quartet
+    # threshold of each derivative order for this list's class mix
+    from ccsd_gpu_b200 import tune
+    tune.enable(not args.no_tune)
+    dshare = float((shells._bas[:, 1][q].max(1) >= 2).mean())
+    heavy = {d: tune.tune_eri_heavy(ds, shells._bas, q_dev, d, dshare) for d in (1, 0)}
     ip1 = lambda: quartet_checksums(ds, q_dev, 1, out=out)   # noqa: E731
     for _ in range(args.warmup):
         ip1()
@@ -681,6 +688,7 @@ def main():
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": "eri_microbench_4096_shells_spd_ip1", "nshell": NSHELL, "quartets_per_rank": nq,
                    "lclasses": int(len(classes)), "schwarz": 1e-12,
+                   "heavy_nf": {"int2e": heavy[0], "ip1": heavy[1], "autotuned": not args.no_tune},
                    "l2": "256 MiB buffer written between steps, outside the per-step kernel events",
                    "parallelism": "dp%d" % ws if ws > 1 else "single"},
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",

@@ -24,7 +24,7 @@ import weakref
 import numpy as np
 import torch
 
-from . import _native
+from . import _native, tune
 
 KIND = {"tf32x3": 0, "bf16x3": 1}
 MODES = ("fp64", "tf32x3", "bf16x3")
@@ -324,7 +324,17 @@ def contract(spec, a, b, out=None, alpha=1.0, beta=0.0, mode="tf32x3", stream=No
     key_n = ("on", tuple(n_idx), so, tuple(out.stride()), tuple(shape_map[i] for i in n_idx))
     om = _dev_offsets(key_m, lambda: _offsets(m_idx, so, shape_map, out), dev)
     on = _dev_offsets(key_n, lambda: _offsets(n_idx, so, shape_map, out), dev)
-    ksplit = _ksplit(m_pad, n_pad, -(-k_pad // _KSTEP[mode]), dev)
+    kblocks = -(-k_pad // _KSTEP[mode])
+    ksplit = _ksplit(m_pad, n_pad, kblocks, dev)
+    if tune.gemm_tuning_active():
+        def trial(s):
+            scratch = torch.empty_strided(out.shape, out.stride(), dtype=torch.float64, device=dev)
+            part = torch.empty(s * M * N, dtype=torch.float64, device=dev) if s > 1 else None
+            _native.call("ccsd_b200_tc_split_gemm", kind, _native.ptr(ahi), _native.ptr(alo), _native.ptr(bhi),
+                         _native.ptr(blo), M, N, m_pad, n_pad, k_pad, _native.ptr(scratch), _native.ptr(om),
+                         _native.ptr(on), float(alpha), 0.0, s, _native.ptr(part), _native.ptr(_Status.get(dev)),
+                         st)
+        ksplit = tune.gemm_split(M, N, K, mode, ksplit, max(1, kblocks // _KB_PER_CHUNK), trial)
     partial = torch.empty(ksplit * M * N, dtype=torch.float64, device=dev) if ksplit > 1 else None
     STATS["flops"] += 2 * M * N * K
     STATS["gemms"] += 1

@@ -1316,13 +1316,16 @@ __global__ void __launch_bounds__(kWarps * 32, 2) eri_s2kl_kernel(
 
 // Explicit quartet list (int4 shells): MODE_QSUM writes two checksums per
 // component per quartet, MODE_GRAD one gamma contraction per component.
+// heavy: quartets with more Cartesian functions than this go to the CTA kernel
+// (0: heavy_nf(D)); the CTA kernel of the same list gets the same value.
 template <int D, bool LOW, int MODE = MODE_QSUM>
 __global__ void __launch_bounds__(kWarps * 32, 2) eri_qsum_kernel(
     const int *__restrict__ atm, const int *__restrict__ bas, const double *__restrict__ env,
     const int4 *__restrict__ quartets, long long nq, double *__restrict__ qsum, int smem_warp,
     const int *__restrict__ ao_loc = nullptr, const double *__restrict__ gamma = nullptr, int nao = 0,
-    double *__restrict__ full = nullptr)
+    double *__restrict__ full = nullptr, int heavy = 0)
 {
+    if (heavy <= 0) heavy = heavy_nf(D);
     extern __shared__ double smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     double *wsm = smem + warp * smem_warp;
@@ -1341,7 +1344,7 @@ __global__ void __launch_bounds__(kWarps * 32, 2) eri_qsum_kernel(
     for (long long t = t0 + warp; t < t1; t += kWarps) {
         const long long q = nq - 1 - t;
         const int4 s = quartets[q];
-        if (quartet_nf(bas, s.x, s.y, s.z, s.w) > heavy_nf(D)) continue;
+        if (quartet_nf(bas, s.x, s.y, s.z, s.w) > heavy) continue;
         double acc[NOUT];
         for (int c = 0; c < NOUT; c++) acc[c] = 0.0;
         HcPlan h;
@@ -1390,8 +1393,9 @@ __global__ void __launch_bounds__(kHeavyThreads, 1) eri_qsum_heavy_kernel(
     const int *__restrict__ atm, const int *__restrict__ bas, const double *__restrict__ env,
     const int4 *__restrict__ quartets, long long nq, double *__restrict__ qsum, int smem_doubles,
     const int *__restrict__ ao_loc = nullptr, const double *__restrict__ gamma = nullptr, int nao = 0,
-    double *__restrict__ full = nullptr)
+    double *__restrict__ full = nullptr, int heavy = 0)
 {
+    if (heavy <= 0) heavy = heavy_nf(D);
     extern __shared__ double smem[];
     S2klOut so = {};
     so.gamma = gamma;
@@ -1401,7 +1405,7 @@ __global__ void __launch_bounds__(kHeavyThreads, 1) eri_qsum_heavy_kernel(
     constexpr int NOUT = MODE == MODE_QSUM ? 2 * NC : NC;
     for (long long q = blockIdx.x; q < nq; q += gridDim.x) {
         const int4 s = quartets[q];
-        if (quartet_nf(bas, s.x, s.y, s.z, s.w) <= heavy_nf(D)) continue;
+        if (quartet_nf(bas, s.x, s.y, s.z, s.w) <= heavy) continue;
         HcPlan h;
         if (LOW && hc_plan(D, bas[s.x * CB_BAS_SLOTS + CB_ANG_OF], bas[s.y * CB_BAS_SLOTS + CB_ANG_OF],
                            bas[s.z * CB_BAS_SLOTS + CB_ANG_OF], bas[s.w * CB_BAS_SLOTS + CB_ANG_OF], h,
@@ -1624,6 +1628,27 @@ int ccsd_b200_eri_s2kl_cart(int deriv, const int32_t *atm, const int32_t *bas, c
     return check_launch("eri_s2kl_kernel");
 }
 
+// Heavy-quartet thresholds of the list entry points (quartet checksums, the
+// ip1 gradient contraction, the dense int2e tensor), per derivative order;
+// set by the autotuner.  The s2kl block entry keeps the compiled values (its
+// heavy list is built by the caller).
+static int g_heavy_list[2] = {kHeavyNf, kHeavyNfIp1};
+
+int ccsd_b200_eri_set_heavy_nf(int deriv, int nf)
+{
+    if (deriv < 0 || deriv > 1 || nf < 1) {
+        set_error("ccsd_b200_eri_set_heavy_nf: invalid argument");
+        return CCSD_B200_ERR_ARG;
+    }
+    g_heavy_list[deriv] = nf;
+    return CCSD_B200_OK;
+}
+
+int ccsd_b200_eri_get_heavy_nf(int deriv)
+{
+    return deriv == 0 || deriv == 1 ? g_heavy_list[deriv] : -1;
+}
+
 int ccsd_b200_eri_quartet_checksums(int deriv, const int32_t *atm, const int32_t *bas, const double *env,
                                     const int32_t *quartets, long long nq, int lmax, double *qsum,
                                     void *stream)
@@ -1637,6 +1662,7 @@ int ccsd_b200_eri_quartet_checksums(int deriv, const int32_t *atm, const int32_t
         return CCSD_B200_ERR_UNSUPPORTED;
     }
     if (nq == 0) return CCSD_B200_OK;
+    const int hv = g_heavy_list[deriv];
     const int sw = smem_per_warp(lmax, deriv);
     const size_t smem = (size_t)sw * kWarps * sizeof(double);
     long long grid = (nq + kWarps - 1) / kWarps;
@@ -1655,7 +1681,8 @@ int ccsd_b200_eri_quartet_checksums(int deriv, const int32_t *atm, const int32_t
         const long long hg = nq < (long long)num_sms() ? nq : (long long)num_sms();
 #define CB_LAUNCH_QSUM_H(DV, LOWV)                                                     \
     if ((rc = prepare_kernel(eri_qsum_heavy_kernel<DV, LOWV>, hsmem))) return rc;       \
-    eri_qsum_heavy_kernel<DV, LOWV><<<(int)hg, kHeavyThreads, hsmem, aux->s>>>(atm, bas, env, q4, nq, qsum, hd);
+    eri_qsum_heavy_kernel<DV, LOWV><<<(int)hg, kHeavyThreads, hsmem, aux->s>>>(atm, bas, env, q4, nq, qsum, hd,    \
+                                                                               nullptr, nullptr, 0, nullptr, hv);
         if (deriv) {
             if (lmax <= 2) { CB_LAUNCH_QSUM_H(1, true) } else { CB_LAUNCH_QSUM_H(1, false) }
         } else {
@@ -1667,7 +1694,8 @@ int ccsd_b200_eri_quartet_checksums(int deriv, const int32_t *atm, const int32_t
     }
 #define CB_LAUNCH_QSUM(DV, LOWV)                                                       \
     if ((rc = prepare_kernel(eri_qsum_kernel<DV, LOWV>, smem))) return rc;              \
-    eri_qsum_kernel<DV, LOWV><<<(int)grid, kWarps * 32, smem, st>>>(atm, bas, env, q4, nq, qsum, sw);
+    eri_qsum_kernel<DV, LOWV><<<(int)grid, kWarps * 32, smem, st>>>(atm, bas, env, q4, nq, qsum, sw, nullptr,    \
+                                                                    nullptr, 0, nullptr, hv);
     if (deriv) {
         if (lmax <= 2) { CB_LAUNCH_QSUM(1, true) } else { CB_LAUNCH_QSUM(1, false) }
     } else {
@@ -1709,13 +1737,14 @@ int ccsd_b200_eri_ip1_contract(const int32_t *atm, const int32_t *bas, const dou
         const long long hg = nq < (long long)num_sms() ? nq : (long long)num_sms();
 #define CB_LAUNCH_GRAD(LOWV)                                                                                      \
     if ((rc = prepare_kernel(eri_qsum_heavy_kernel<1, LOWV, MODE_GRAD>, hsmem))) return rc;                       \
-    eri_qsum_heavy_kernel<1, LOWV, MODE_GRAD><<<(int)hg, kHeavyThreads, hsmem, aux->s>>>(atm, bas, env, q4, nq,   \
-                                                                                      qwork, hd, ao_loc, gamma, nao); \
+    eri_qsum_heavy_kernel<1, LOWV, MODE_GRAD><<<(int)hg, kHeavyThreads, hsmem, aux->s>>>(                         \
+        atm, bas, env, q4, nq, qwork, hd, ao_loc, gamma, nao, nullptr, g_heavy_list[1]);                          \
     if ((rc = check_launch("eri_qsum_heavy_kernel<grad>"))) return rc;                                            \
     cudaEventRecord(aux->join, aux->s);                                                                            \
     if ((rc = prepare_kernel(eri_qsum_kernel<1, LOWV, MODE_GRAD>, smem))) return rc;                              \
     eri_qsum_kernel<1, LOWV, MODE_GRAD><<<(int)grid, kWarps * 32, smem, st>>>(atm, bas, env, q4, nq, qwork, sw,     \
-                                                                            ao_loc, gamma, nao);
+                                                                            ao_loc, gamma, nao, nullptr,            \
+                                                                            g_heavy_list[1]);
         if (lmax <= 2) { CB_LAUNCH_GRAD(true) } else { CB_LAUNCH_GRAD(false) }
 #undef CB_LAUNCH_GRAD
         cudaStreamWaitEvent(st, aux->join, 0);
@@ -1755,12 +1784,13 @@ int ccsd_b200_eri_full_cart(const int32_t *atm, const int32_t *bas, const double
 #define CB_LAUNCH_FULL(LOWV)                                                                                      \
     if ((rc = prepare_kernel(eri_qsum_heavy_kernel<0, LOWV, MODE_FULL>, hsmem))) return rc;                       \
     eri_qsum_heavy_kernel<0, LOWV, MODE_FULL><<<(int)hg, kHeavyThreads, hsmem, aux->s>>>(                        \
-        atm, bas, env, q4, nq, nullptr, hd, ao_loc, nullptr, nao, out);                                         \
+        atm, bas, env, q4, nq, nullptr, hd, ao_loc, nullptr, nao, out, g_heavy_list[0]);                        \
     if ((rc = check_launch("eri_qsum_heavy_kernel<full>"))) return rc;                                            \
     cudaEventRecord(aux->join, aux->s);                                                                            \
     if ((rc = prepare_kernel(eri_qsum_kernel<0, LOWV, MODE_FULL>, smem))) return rc;                              \
     eri_qsum_kernel<0, LOWV, MODE_FULL><<<(int)grid, kWarps * 32, smem, st>>>(atm, bas, env, q4, nq, nullptr, sw,   \
-                                                                             ao_loc, nullptr, nao, out);
+                                                                             ao_loc, nullptr, nao, out,             \
+                                                                             g_heavy_list[0]);
     if (lmax <= 2) { CB_LAUNCH_FULL(true) } else { CB_LAUNCH_FULL(false) }
 #undef CB_LAUNCH_FULL
     cudaStreamWaitEvent(st, aux->join, 0);

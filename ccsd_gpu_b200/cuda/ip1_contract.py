@@ -8,10 +8,12 @@ in memory and contracts it with the 2-RDM and the HF density products
 contracts it with Gamma inside the kernel; only three numbers per quartet
 leave the SM, and a fixed-order segment sum turns them into per-atom values.
 """
+from types import SimpleNamespace
+
 import numpy as np
 import torch
 
-from .. import _native
+from .. import _native, tune
 from .basis import _check_mol, get_basis_cached, upload_geometry
 
 
@@ -86,6 +88,9 @@ def contract_int2e_ip1(mol, gamma, stream=None):
     atm, env = upload_geometry(mol, dev)
     q, seg = gradient_quartets(topo, mol.natm)
     nq = int(q.shape[0])
+    if nq:
+        ds = SimpleNamespace(atm=atm, bas=topo.bas_dev, env=env, lmax=topo.lmax)
+        tune.tune_eri_heavy(ds, topo.dc_bas, q, 1, tune.basis_dshare(topo.dc_bas))
     qwork = torch.empty((max(nq, 1), 3), dtype=torch.float64, device=dev)
     out = torch.empty((mol.natm, 3), dtype=torch.float64, device=dev)
     _native.call("ccsd_b200_eri_ip1_contract", _native.ptr(atm), _native.ptr(topo.bas_dev), _native.ptr(env),

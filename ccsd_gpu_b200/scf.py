@@ -8,10 +8,12 @@ eigen-solves are FP64 on the device.  The object exposes the attributes the
 CCSD gradient reads from a PySCF RHF: mol, mo_energy, mo_coeff, mo_occ, e_tot,
 make_rdm1, get_ovlp, get_hcore, get_veff, energy_nuc.
 """
+from types import SimpleNamespace
+
 import numpy as np
 import torch
 
-from . import _native
+from . import _native, tune
 from .cuda.basis import _check_mol, get_basis_cached, upload_geometry
 from .int1e import intor1e
 
@@ -47,6 +49,8 @@ def full_eri_gpu(mol):
     atm, env = upload_geometry(mol, dev)
     q = unique_quartets(topo)
     n = topo.nao_cart
+    tune.tune_eri_heavy(SimpleNamespace(atm=atm, bas=topo.bas_dev, env=env, lmax=topo.lmax), topo.dc_bas, q, 0,
+                        tune.basis_dshare(topo.dc_bas))
     g = torch.empty((n, n, n, n), dtype=torch.float64, device=dev)
     _native.call("ccsd_b200_eri_full_cart", _native.ptr(atm), _native.ptr(topo.bas_dev), _native.ptr(env),
                  _native.ptr(topo.ao_loc_dev), n, _native.ptr(q), int(q.shape[0]), topo.lmax, _native.ptr(g),

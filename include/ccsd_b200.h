@@ -66,6 +66,19 @@ int ccsd_b200_eri_quartet_checksums(int deriv, const int32_t *atm, const int32_t
                                     void *stream);
 
 /*
+ * Heavy-quartet threshold of the list entry points (quartet checksums,
+ * ccsd_b200_eri_ip1_contract, ccsd_b200_eri_full_cart) for derivative order
+ * deriv (0 or 1): quartets whose Cartesian block has more than nf functions
+ * run on the CTA-cooperative kernel, the others one warp each.  Defaults
+ * 1000 (int2e) and 500 (int2e_ip1); set by the autotuner (process-wide, all
+ * devices).  The get call returns the current value, -1 for a bad deriv.  No
+ * counterpart in the reference (its launch shape is fixed,
+ * ref: ccsd_gpu/cuda/int2e_ip1_gpu.py:148-216).
+ */
+int ccsd_b200_eri_set_heavy_nf(int deriv, int nf);
+int ccsd_b200_eri_get_heavy_nf(int deriv);
+
+/*
  * Cartesian -> spherical transform of an s2kl block:
  * cart (ncomp, nfc, naoc, naoc(naoc+1)/2) -> out (ncomp, nfs, naos, naos(naos+1)/2),
  * tmp (ncomp, nfs, naos, naoc(naoc+1)/2) is caller-provided scratch.  The
