@@ -123,7 +123,7 @@ def basis_dshare(bas):
     return 1.0 - float((bas[:, 1] < 2).mean()) ** 4
 
 
-def tune_eri_heavy(ds, bas, quartets, deriv, dshare, sample=1 << 15, candidates=None, timer=None):
+def tune_eri_heavy(ds, bas, quartets, deriv, dshare, sample=1 << 17, candidates=None, timer=None):
     """Choose and set the heavy threshold for lists like ``quartets`` (an
     (nq, 4) int32 CUDA tensor over the shells of ``ds``: an object with
     device ``atm``, ``bas``, ``env`` and ``lmax``; ``bas`` is the host copy).
