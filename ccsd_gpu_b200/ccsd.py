@@ -221,10 +221,13 @@ class CCSD:
                     adiis = DIIS(self.diis_space)
                     e_old = e
                     continue
-                self.converged = True
+                # converged only if the requested tolerance was met: a split-precision
+                # solve stopped at its noise floor without the FP64 polish is not
+                self.converged = normt < self.conv_tol_normt
                 break
             e_old = e
         check_status()
+        self.normt = self._t_history[-1][1] if self._t_history else None
         self.e_corr = e
         self.t1, self.t2 = host_copy(t1), host_copy(t2)
         remember_device(self, "t1", self.t1, t1)

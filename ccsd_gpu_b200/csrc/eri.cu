@@ -19,6 +19,7 @@
 #include "common.cuh"
 #include "rys.cuh"
 
+#include <atomic>
 #include <stdarg.h>
 #include <stdio.h>
 #include <string.h>
@@ -1849,24 +1850,31 @@ int ccsd_b200_cart2sph_s2kl(const double *cart, double *tmp, double *out, int nc
 static constexpr long long kC2sScratchDoubles = 4ll << 20;
 static __device__ __align__(256) double g_c2s_scratch[kC2sScratchDoubles];
 
+// The cached address belongs to the device's primary context, which this
+// library assumes lives for the whole process (a cudaDeviceReset creates a new
+// context with a new address; call nothing here after one).  First calls from
+// several host threads may each look the address up; they store the same
+// value, through an atomic, so the cache is free of data races.
 static int c2s_scratch_address(double **out)
 {
-    static double *addr[64] = {};
+    static std::atomic<double *> addr[64];
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
         set_error("ccsd_b200_cart2sph_s2kl_noalloc: no current CUDA device");
         return CCSD_B200_ERR_LAUNCH;
     }
-    if (!addr[dev]) {
+    double *a = addr[dev].load(std::memory_order_acquire);
+    if (!a) {
         void *p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_c2s_scratch);
         if (e != cudaSuccess || !p) {
             set_error("ccsd_b200_cart2sph_s2kl_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
             return CCSD_B200_ERR_LAUNCH;
         }
-        addr[dev] = static_cast<double *>(p);
+        a = static_cast<double *>(p);
+        addr[dev].store(a, std::memory_order_release);
     }
-    *out = addr[dev];
+    *out = a;
     return CCSD_B200_OK;
 }
 

@@ -103,6 +103,18 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *s
     return false;
 }
 
+// Bounded wait used on the abort path only: waits for the asynchronous work
+// this thread has already issued (TMA loads, tcgen05.mma) to land, whatever
+// other CTAs recorded in `status`.  Returns false after `limit_ns`.
+__device__ __forceinline__ bool mbar_settle(uint64_t *bar, uint32_t parity, unsigned long long limit_ns = TC_WAIT_NS)
+{
+    const unsigned long long t0 = global_ns();
+    for (unsigned it = 0;; it++) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((it & 63) == 63 && global_ns() - t0 > limit_ns) return false;
+    }
+}
+
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar)
 {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
@@ -191,7 +203,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_split_gemm_kernel(
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     __shared__ __align__(8) uint64_t full_bar[TC_STAGES], empty_bar[TC_STAGES], accf_bar[2], acce_bar[2];
     __shared__ uint32_t tmem_base_s;
+    __shared__ int abort_s;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // A wait already expired in this or an earlier GEMM (the status is sticky
+    // until the host reads it): leave before any TMEM allocation or TMA, with
+    // the outputs untouched.  The decision is made once for the whole CTA.
+    if (threadIdx.x == 0) abort_s = *(volatile int *)status;
+    __syncthreads();
+    if (abort_s) return;
     // raster: groups of TC_GROUP_M row tiles, row tile fastest inside a group, so
     // the CTAs resident at one time share a few A row tiles and each B tile is
     // fetched from HBM about once
@@ -236,6 +255,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_split_gemm_kernel(
     if (warp == 0) {
         if (lane == 0) {
             // ---- TMA producer
+            int issued = 0;
             for (int kb = 0; kb < nkb; kb++) {
                 const int s = kb % TC_STAGES;
                 const uint32_t ph = (kb / TC_STAGES) & 1;
@@ -247,13 +267,20 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_split_gemm_kernel(
                 tma_load_2d(&map_alo, &full_bar[s], st + TC_TILE_BYTES, kx, m0);
                 tma_load_2d(&map_bhi, &full_bar[s], st + 2 * TC_TILE_BYTES, kx, n0);
                 tma_load_2d(&map_blo, &full_bar[s], st + 3 * TC_TILE_BYTES, kx, n0);
+                issued = kb + 1;
             }
+            // The last TC_STAGES loads may not have been consumed (abort, or the
+            // normal end): the CTA must not exit with bulk copies in flight into
+            // its shared memory, so wait (bounded) until each of them has landed.
+            for (int kb = issued > TC_STAGES ? issued - TC_STAGES : 0; kb < issued; kb++)
+                mbar_settle(&full_bar[kb % TC_STAGES], (kb / TC_STAGES) & 1);
         }
     } else if (warp == 1) {
         if (lane == 0) {
             // ---- MMA issuer
             const uint32_t idesc = instr_desc<KIND>();
             bool ok = true;
+            int last = -1;                          // chunk of the last accf commit
             for (int c = 0; c < nchunks && ok; c++) {
                 const int buf = c & 1;
                 const uint32_t use = (uint32_t)(c >> 1);
@@ -280,7 +307,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_split_gemm_kernel(
                     umma_commit(&empty_bar[s]);     // stage reusable once these MMAs finish
                 }
                 umma_commit(&accf_bar[buf]);        // chunk accumulated (also on the error path)
+                last = c;
             }
+            // TMEM is freed at the end of the kernel: every MMA issued here must
+            // have completed first.  The last commit tracks all of them.
+            if (last >= 0) mbar_settle(&accf_bar[last & 1], ((uint32_t)(last >> 1)) & 1);
         }
     } else {
         // ---- drain warps: FP64 running sums in registers, one write at the end

@@ -26,7 +26,7 @@ import numpy as np
 import torch
 
 from . import _native
-from .contract import contract
+from .contract import check_status, contract
 from .gpu_ccsd_lambda import device_amp
 from .cuda.ip1_contract import contract_int2e_ip1
 from .int1e import intor1e
@@ -266,6 +266,10 @@ def grad_elec_gpu(mycc, t1, t2, l1, l2, atmlst=None, verbose=None):
         de[a] -= torch.einsum("xij,ij->x", s1a, zeta[p0:p1_])
         de[a] -= torch.einsum("xji,ij->x", s1a, zeta[:, p0:p1_])
         de[a] -= 2 * torch.einsum("xij,ij->x", s1a, vhf_s1occ[p0:p1_])
+    # the RDM and gvovv contractions ran on the tensor cores: an expired
+    # pipeline wait leaves their tiles unwritten, so raise instead of
+    # returning a gradient built from them
+    check_status(dev)
     return de[list(atmlst)].cpu().numpy()
 
 
@@ -333,6 +337,7 @@ def compute_ml_ccsd_forces_gpu(mf, t1, t2, l1, l2, precision="tf32x3"):
     mycc.t1, mycc.t2, mycc.l1, mycc.l2 = t1, t2, l1, l2
     mycc.converged = mycc.converged_lambda = True
     de = grad_elec_gpu(mycc, t1, t2, l1, l2)
+    check_status()
     return np.array(de + mf.nuc_grad_method().grad_nuc())
 
 

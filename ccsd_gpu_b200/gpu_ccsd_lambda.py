@@ -377,10 +377,15 @@ def kernel_gpu(mycc, eris=None, t1=None, t2=None, l1=None, l2=None, max_cycle=No
                 step = make_step(imds, cur_mode)
                 adiis = DIIS(space) if use_diis else None
                 continue
-            conv = normt < tol or (cur_mode != "fp64" and not polish)
+            # converged only if the requested tolerance was met: a split-precision
+            # solve stopped at its noise floor without the FP64 polish is not
+            conv = normt < tol
             break
     check_status()
     mycc._lambda_history = history
+    # achieved update norm of the last iteration (the reference records only
+    # the flag, ccsd_gpu/gpu_ccsd_lambda.py:445-448)
+    mycc.lambda_normt = history[-1][1] if history else None
     mycc._last_lambda_dev = (l1g, l2g)
     return conv, host_copy(l1g), host_copy(l2g)
 

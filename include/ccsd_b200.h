@@ -105,9 +105,11 @@ int ccsd_b200_cart2sph_s2kl(const double *cart, double *tmp, double *out, int nc
  * process exits.  Larger blocks are rejected with CCSD_B200_ERR_ARG and a
  * message giving both sizes.  The first call on a device looks up the array's
  * address (cudaGetSymbolAddress) and must come before any stream capture.
- * All calls share the array, so calls that overlap on the GPU race and must
- * be serialised by the caller.  Allocates nothing; arguments and result as in
- * ccsd_b200_cart2sph_s2kl.
+ * The address is cached per device and belongs to the device's primary
+ * context, which is assumed to live for the whole process (do not call this
+ * after a cudaDeviceReset).  All calls share the array, so calls that overlap
+ * on the GPU race and must be serialised by the caller.  Allocates nothing;
+ * arguments and result as in ccsd_b200_cart2sph_s2kl.
  */
 int ccsd_b200_cart2sph_s2kl_noalloc(const double *cart, double *out, int ncomp, int nfc, int naoc, int nfs,
                                     int naos, const int32_t *ptr_i, const int32_t *idx_i, const double *val_i,

@@ -1,7 +1,8 @@
 """ORACLE recipe: build the reference's ERI kernels for the CPU into oracle/_ref/.
 
-Runs only where the reference checkout exists (``REF_ROOT``, default
-``/root/reference``).  It imports the reference's kernel-source modules
+Runs only where the reference checkout exists; its path is an argument
+(``build(ref_root)``, or the first command-line argument, or ``REF_ROOT``):
+there is no default location.  It imports the reference's kernel-source modules
 (ccsd_gpu/cuda/int2e_ip1_module.py, ccsd_gpu/cuda/int2e_module.py) with a
 stand-in for ``cupy`` (only ``_build_cuda_source`` and the Rys data loader are
 called, no CuPy object is touched), writes the generated kernel source to
@@ -54,8 +55,11 @@ def generate_sources(ref_root):
 
 
 def build(ref_root=None, verbose=False):
-    ref_root = ref_root or os.environ.get("REF_ROOT", "/root/reference")
-    if not os.path.isdir(os.path.join(ref_root, "ccsd_gpu", "cuda")):
+    """Build oracle/_ref/libref_eri.so from the checkout at ``ref_root``
+    (``REF_ROOT`` if None).  Returns None when no checkout is given or it has
+    no ccsd_gpu/cuda directory (the prebuilt library, if any, is kept)."""
+    ref_root = ref_root or os.environ.get("REF_ROOT")
+    if not ref_root or not os.path.isdir(os.path.join(ref_root, "ccsd_gpu", "cuda")):
         return None
     os.makedirs(OUT, exist_ok=True)
     src_eri, src_ip1 = generate_sources(ref_root)
@@ -73,4 +77,7 @@ def build(ref_root=None, verbose=False):
 
 
 if __name__ == "__main__":
-    print(build(sys.argv[1] if len(sys.argv) > 1 else None, verbose=True))
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("REF_ROOT")
+    if not root:
+        sys.exit("usage: python oracle/build_ref.py <reference checkout>   (or set REF_ROOT)")
+    print(build(root, verbose=True))

@@ -11,7 +11,8 @@ stand-ins below are the minimum those modules touch on the exercised paths:
     ``_add_vvvv(None, l2, eris, with_ovvv=False, t2sym='jiba')`` performs.
 Inputs: a synthetic closed-shell state (nocc=4, nvir=9) with 8-fold symmetric
 MO integrals and a non-diagonal Fock matrix, seed 0.
-Run from the repository root:  python tests/golden/make_cc_golden.py
+Run from the repository root:
+    python tests/golden/make_cc_golden.py <reference checkout>   (or set REF_ROOT)
 """
 import importlib.util
 import os
@@ -21,7 +22,6 @@ import types
 import numpy as np
 
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
-REF = os.environ.get("REF_ROOT", "/root/reference")
 OUT = os.path.join(ROOT, "tests", "golden", "cc_small.npz")
 
 
@@ -117,7 +117,15 @@ def synthetic_state(nocc=4, nvir=9, seed=0):
     return dict(g=g, fock=fock, mo_energy=e, t1=t1, t2=t2, l1=l1, l2=l2, eris=eris, mo_coeff=mo_coeff)
 
 
+def ref_root():
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("REF_ROOT")
+    if not root or not os.path.isdir(os.path.join(root, "ccsd_gpu")):
+        sys.exit("usage: python %s <reference checkout>   (or set REF_ROOT)" % sys.argv[0])
+    return root
+
+
 def main():
+    REF = ref_root()
     _stub_modules()
     lam = _load("ref_gpu_ccsd_lambda", os.path.join(REF, "ccsd_gpu", "gpu_ccsd_lambda.py"))
     grd = _load("ref_gpu_ccsd_grad", os.path.join(REF, "ccsd_gpu", "gpu_ccsd_grad.py"))

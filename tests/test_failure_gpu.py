@@ -6,6 +6,7 @@ same wait on a barrier nothing arrives at: the host must see the code, and
 the context must stay usable for the next contraction."""
 import time
 
+import numpy as np
 import pytest
 import torch
 
@@ -45,3 +46,27 @@ def test_contract_status_raises_after_expired_wait():
     with pytest.raises(_native.NativeError):
         check_status()
     check_status()          # reset to 0 by the raise
+
+
+def test_gradient_raises_after_expired_wait(monkeypatch):
+    """grad_elec_gpu must not return a gradient assembled from tensor-core
+    tiles that an expired wait left unwritten: with the status already set
+    the GEMMs of the gradient leave their outputs untouched and the call raises."""
+    import ccsd_gpu_b200.contract as C
+    from ccsd_gpu_b200 import _native
+    from ccsd_gpu_b200.ccsd import CCSD
+    from ccsd_gpu_b200.gto import M
+    from ccsd_gpu_b200.scf import RHF
+    monkeypatch.setattr(C, "SMALL_FLOPS", 0.0)
+    monkeypatch.setattr(C, "MIXED_MIN_LADDER_FLOPS", 0.0)
+    mol = M(atom="O 0 0 0; H 0 -0.757 0.587; H 0 0.757 0.587", basis="sto-3g")
+    cc = CCSD(RHF(mol).run(), precision="tf32x3")
+    cc.kernel()
+    cc.solve_lambda()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    _native.call("ccsd_b200_wait_probe", _native.ptr(C._Status.get(dev)), 20_000_000, 5, _native.stream())
+    with pytest.raises(_native.NativeError):
+        cc.nuc_grad_method().kernel()
+    C.check_status()            # reset by the raise
+    g = cc.nuc_grad_method().kernel()
+    assert np.isfinite(g).all() and np.abs(g.sum(0)).max() < 1e-8

@@ -80,7 +80,11 @@ def test_ccsd_gradient_matches_oracle(h2o_oracle, mode, polish, tol):
     cc.conv_tol_normt = 1e-9
     cc.lambda_polish = polish
     cc.solve_lambda()
-    assert cc.converged_lambda
+    if polish or mode == "fp64":
+        assert cc.converged_lambda
+    else:
+        # stopped at the split-precision floor: not converged to 1e-9, and says so
+        assert not cc.converged_lambda and cc.lambda_normt < 1e-6
     g = cc.nuc_grad_method().kernel()
     assert np.abs(g - h2o_oracle["grad"]).max() < tol
     assert np.abs(g.sum(0)).max() < 1e-8

@@ -71,3 +71,18 @@ def test_solve_lambda_converges_to_oracle_fixed_point(gold, mode):
     assert cc.converged_lambda
     tol = 1e-9 if mode == "fp64" else 1e-6
     assert rel(l1, ref1) < tol and rel(l2, ref2) < tol
+
+
+def test_split_precision_without_polish_reports_not_converged(gold):
+    """A split-precision solve that stops at its noise floor (polish off) must
+    not claim the requested 1e-10 (the reference's converged_lambda contract,
+    ccsd_gpu/gpu_ccsd_lambda.py:445-448); the achieved norm is recorded."""
+    from ccsd_gpu_b200.gpu_ccsd_lambda import MIXED_FLOOR, solve_lambda_gpu
+    cc = SimpleNamespace(t1=gold["t1"], t2=gold["t2"], max_cycle=100, conv_tol_normt=1e-10, level_shift=0.0,
+                         precision="tf32x3", lambda_polish=False)
+    solve_lambda_gpu(cc, eris=gold["eris"])
+    assert cc.converged_lambda is False
+    assert cc.lambda_normt < MIXED_FLOOR
+    cc.lambda_polish = True
+    solve_lambda_gpu(cc, eris=gold["eris"])
+    assert cc.converged_lambda is True and cc.lambda_normt < 1e-10
