@@ -216,16 +216,22 @@ def fci_2e(mf):
 
 
 def grad_elec(mf, t1, t2, l1, l2, eri_ip1=None):
-    """CCSD electronic gradient (natm, 3), restating grad_elec_gpu step by step."""
+    """CCSD electronic gradient (natm, 3), restating grad_elec_gpu step by step.
+
+    Frozen core orbitals (no frozen virtuals) are taken from the amplitude
+    shapes: the RDMs live on the active orbitals and the frozen-active block
+    of the relaxed density is Imat / (e_F - e_A) (ref: ccsd_gpu/gpu_ccsd_grad.py:373-378,510-518)."""
     mol = mf.mol
     Cm, e, occ = mf.mo_coeff, mf.mo_energy, mf.mo_occ
     nocc = int((occ > 0).sum())
     nao, nmo = Cm.shape
+    nf = nocc - t1.shape[0]
+    Ca = Cm[:, nf:]
     eri = mf.eri
     ip1 = full_eri_ip1(mol) if eri_ip1 is None else eri_ip1
     doo, dov, dvo, dvv = C.gamma1(t1, t2, l1, l2)
     d2 = C.gamma2(t1, t2, l1, l2)
-    dm2 = es("pi,qj,rk,sl,ijkl->pqrs", Cm, Cm, Cm, Cm, C.rdm2_mo(d2))
+    dm2 = es("pi,qj,rk,sl,ijkl->pqrs", Ca, Ca, Ca, Ca, C.rdm2_mo(d2))
     dm2 = dm2 + dm2.transpose(1, 0, 2, 3)
     dm2 = 0.5 * (dm2 + dm2.transpose(0, 1, 3, 2))
     P = 2 * Cm[:, :nocc] @ Cm[:, :nocc].T
@@ -247,8 +253,12 @@ def grad_elec(mf, t1, t2, l1, l2, eri_ip1=None):
     S = mf.S
     Imat = Cm.T @ Imat @ S @ Cm * -1
     dm1mo = np.zeros((nmo, nmo))
-    dm1mo[:nocc, :nocc] = doo + doo.T
+    dm1mo[nf:nocc, nf:nocc] = doo + doo.T
     dm1mo[nocc:, nocc:] = dvv + dvv.T
+    if nf:
+        dco = Imat[:nf, nf:nocc] / (e[:nf, None] - e[None, nf:nocc])
+        dm1mo[:nf, nf:nocc] = dco
+        dm1mo[nf:nocc, :nf] = dco.T
     dm1 = Cm @ dm1mo @ Cm.T
     vhf = veff(eri, dm1) * 2
     Xvo = Cm[:, nocc:].T @ vhf @ Cm[:, :nocc] + Imat[:nocc, nocc:].T - Imat[nocc:, :nocc]

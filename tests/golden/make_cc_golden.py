@@ -9,8 +9,14 @@ stand-ins below are the minimum those modules touch on the exercised paths:
     ``pyscf.cc._ccsd.make_tau`` (t2 + t1 (x) t1), ``pyscf.cc.ccsd.BLKMIN``;
   * ``mycc._add_vvvv`` = sum_cd l2[i,j,c,d] (ac|bd), the operation PySCF's
     ``_add_vvvv(None, l2, eris, with_ovvv=False, t2sym='jiba')`` performs.
-Inputs: a synthetic closed-shell state (nocc=4, nvir=9) with 8-fold symmetric
-MO integrals and a non-diagonal Fock matrix, seed 0.
+Inputs: synthetic closed-shell states with 8-fold symmetric MO integrals and a
+non-diagonal Fock matrix:
+  * cc_small.npz    nocc=4, nvir=9, seed 0, one virtual block;
+  * cc_blocked.npz  nocc=5, nvir=10, seed 1, with ``memGetInfo`` reporting
+    almost no free memory, so the reference's _gpu_block_size
+    (ccsd_gpu/gpu_ccsd_lambda.py:54-61) returns BLKMIN = 4 and every blocked
+    loop of make_intermediates_gpu / update_lambda_gpu takes several blocks
+    (virtual blocks 4+4+2, occupied blocks 4+1).
 Run from the repository root:
     python tests/golden/make_cc_golden.py <reference checkout>   (or set REF_ROOT)
 """
@@ -23,6 +29,8 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 OUT = os.path.join(ROOT, "tests", "golden", "cc_small.npz")
+OUT_BLOCKED = os.path.join(ROOT, "tests", "golden", "cc_blocked.npz")
+FREE_BYTES = [1 << 40]       # what the cupy stand-in's memGetInfo reports
 
 
 def _stub_modules():
@@ -32,7 +40,7 @@ def _stub_modules():
         setattr(cp, name, getattr(np, name))
     cp.asnumpy = np.asarray
     cp.ndarray = np.ndarray
-    rt = types.SimpleNamespace(memGetInfo=lambda: (1 << 40, 1 << 40), getDeviceCount=lambda: 1)
+    rt = types.SimpleNamespace(memGetInfo=lambda: (FREE_BYTES[0], 1 << 40), getDeviceCount=lambda: 1)
     cp.cuda = types.SimpleNamespace(runtime=rt, Device=lambda: types.SimpleNamespace(id=0))
 
     pyscf = types.ModuleType("pyscf")
@@ -129,7 +137,13 @@ def main():
     _stub_modules()
     lam = _load("ref_gpu_ccsd_lambda", os.path.join(REF, "ccsd_gpu", "gpu_ccsd_lambda.py"))
     grd = _load("ref_gpu_ccsd_grad", os.path.join(REF, "ccsd_gpu", "gpu_ccsd_grad.py"))
-    s = synthetic_state()
+    FREE_BYTES[0] = 1 << 40
+    run(lam, grd, synthetic_state(), OUT)
+    FREE_BYTES[0] = 1
+    run(lam, grd, synthetic_state(5, 10, seed=1), OUT_BLOCKED)
+
+
+def run(lam, grd, s, path):
     eris = s["eris"]
     mycc = types.SimpleNamespace(stdout=None, verbose=0, max_memory=1e9, level_shift=0.0)
     mycc._add_vvvv = lambda t1, t2, e, with_ovvv=False, t2sym=None: np.einsum("ijcd,acbd->ijab", t2, e.vvvv)
@@ -147,8 +161,8 @@ def main():
     for k, v in zip(("dovov", "dvvvv", "doooo", "doovv", "dovvo", "dvvov", "dovvv", "dooov"), d2):
         if v is not None:
             out[k] = v
-    np.savez_compressed(OUT, **out)
-    print(OUT, os.path.getsize(OUT))
+    np.savez_compressed(path, **out)
+    print(path, os.path.getsize(path))
 
 
 if __name__ == "__main__":

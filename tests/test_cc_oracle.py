@@ -9,9 +9,11 @@ from oracle import cc_oracle as C
 from tests.conftest import GOLDEN
 
 
-@pytest.fixture(scope="module")
-def gold():
-    return dict(np.load(os.path.join(GOLDEN, "cc_small.npz")))
+# cc_small: one virtual block in the reference's loops; cc_blocked: the
+# reference ran with several virtual and occupied blocks
+@pytest.fixture(scope="module", params=["cc_small.npz", "cc_blocked.npz"])
+def gold(request):
+    return dict(np.load(os.path.join(GOLDEN, request.param)))
 
 
 def rel(a, b):

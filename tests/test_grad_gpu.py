@@ -51,11 +51,12 @@ def test_ccsd_energy_matches_oracle(h2o_oracle, mode, tol):
     assert abs(cc.e_tot - h2o_oracle["etot"]) < tol
 
 
+@pytest.mark.parametrize("fixture", ["cc_small.npz", "cc_blocked.npz"])
 @pytest.mark.parametrize("mode,tol", [("fp64", 1e-12), ("tf32x3", 5e-6)])
-def test_rdm_intermediates_match_reference_golden(mode, tol):
+def test_rdm_intermediates_match_reference_golden(mode, tol, fixture):
     from types import SimpleNamespace
     from ccsd_gpu_b200 import gpu_ccsd_grad as G
-    d = dict(np.load(os.path.join(GOLDEN, "cc_small.npz")))
+    d = dict(np.load(os.path.join(GOLDEN, fixture)))
     cc = SimpleNamespace(precision=mode)
     args = (d["t1"], d["t2"], d["l1"], d["l2"])
     rel = lambda a, b: float(np.abs(a.cpu().numpy() - b).max() / np.abs(b).max())   # noqa: E731

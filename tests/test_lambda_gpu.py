@@ -23,9 +23,9 @@ def _tensor_cores_at_small_sizes(monkeypatch):
     monkeypatch.setattr(Cn, "MIXED_MIN_LADDER_FLOPS", 0.0)
 
 
-@pytest.fixture(scope="module")
-def gold():
-    d = dict(np.load(os.path.join(GOLDEN, "cc_small.npz")))
+@pytest.fixture(scope="module", params=["cc_small.npz", "cc_blocked.npz"])
+def gold(request):
+    d = dict(np.load(os.path.join(GOLDEN, request.param)))
     eris = C.mo_blocks(d["g"], d["t1"].shape[0])
     d["eris"] = SimpleNamespace(fock=d["fock"], mo_energy=d["mo_energy"], **vars(eris))
     return d
