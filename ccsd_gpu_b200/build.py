@@ -35,6 +35,7 @@ def sources():
 
 def headers():
     return sorted(glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.inc"))
+                  + glob.glob(os.path.join(CSRC, "*.h"))
                   + glob.glob(os.path.join(HERE, "..", "include", "*.h")))
 
 

@@ -31,4 +31,14 @@ int check_launch(const char *what);
 
 __host__ __device__ __forceinline__ int ncart(int l) { return (l + 1) * (l + 2) / 2; }
 
+// pair index p = k (k + 1) / 2 + l (k >= l) -> (k, l)
+__device__ __forceinline__ void decode_pair(long long p, int &k, int &l)
+{
+    int kk = (int)((sqrt(8.0 * (double)p + 1.0) - 1.0) * 0.5);
+    while ((long long)kk * (kk + 1) / 2 > p) kk--;
+    while ((long long)(kk + 1) * (kk + 2) / 2 <= p) kk++;
+    k = kk;
+    l = (int)(p - (long long)kk * (kk + 1) / 2);
+}
+
 }  // namespace cb

@@ -1,0 +1,46 @@
+// Launchers of the ERI kernels (eri_kernels.cuh), instantiated per
+// (derivative order D, LOW = all shells l <= 2) in the eri_inst_*.cu units.
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+namespace cb {
+
+static constexpr int kWarps = 4;          // warps (quartets in flight) per CTA of the warp kernels
+static constexpr int kHeavyThreads = 256; // threads of the CTA (heavy-quartet) kernels
+static constexpr int kMaxSlots = 64;      // slots per batch cap
+static constexpr int kParStride = 12;     // doubles of per-slot parameters
+static constexpr int kHcSmem = 3072;      // doubles of shared memory per warp on the contracted-HRR path
+
+// Quartets whose Cartesian block has more functions than heavy_nf(D) go to
+// the CTA-cooperative kernel; smaller ones are one warp each.  Measured on the
+// 2^18-quartet benchmark set: int2e is fastest with the (dd|dp)-class blocks
+// (648 functions) on warps, int2e_ip1 with them on CTAs (119 -> 89 ms).
+static constexpr int kHeavyNf = 1000;
+static constexpr int kHeavyNfIp1 = 500;
+__host__ __device__ constexpr int heavy_nf(int D) { return D ? kHeavyNfIp1 : kHeavyNf; }
+
+enum { MODE_S2KL = 0, MODE_QSUM = 1, MODE_GRAD = 2, MODE_FULL = 3 };
+
+struct EriArgs {
+    const int *atm = nullptr, *bas = nullptr;
+    const double *env = nullptr;
+    const int *ao_loc = nullptr;
+    int ish0 = 0, ish1 = 0, nbas = 0, nao = 0;    // s2kl block
+    double *out = nullptr;                         // s2kl output
+    const int4 *quartets = nullptr;                // explicit list (or the s2kl heavy list)
+    long long nq = 0;
+    double *qsum = nullptr;                        // per-quartet checksums / gradient values
+    const double *gamma = nullptr;                 // MODE_GRAD density
+    double *full = nullptr;                        // MODE_FULL dense tensor
+    int heavy = 0;                                 // heavy-quartet threshold (0: compiled default)
+    int smem_warp = 0, smem_heavy = 0;             // doubles of shared memory per warp / per heavy CTA
+};
+
+template <int D, bool LOW> int launch_s2kl(const EriArgs &a, long long grid, size_t smem, cudaStream_t st);
+template <int D, bool LOW> int launch_s2kl_heavy(const EriArgs &a, long long grid, size_t smem, cudaStream_t st);
+template <int D, bool LOW, int MODE> int launch_list(const EriArgs &a, long long grid, size_t smem, cudaStream_t st);
+template <int D, bool LOW, int MODE>
+int launch_list_heavy(const EriArgs &a, long long grid, size_t smem, cudaStream_t st);
+
+}  // namespace cb
