@@ -140,6 +140,101 @@ __device__ __forceinline__ void kept_pair(const PairMask &m, int k, int &ia, int
     ib = t - ia * m.nb;
 }
 
+
+// ---- Gaussian-product data of the kept primitive pairs (phase A, part 1) ----
+// One row of kPairStride doubles per kept primitive pair of a shell pair
+// (a, b), with R = A - B and r2 = |R|^2:
+//   [0..2] P - A = -b/(a+b) R,  [3] a+b,  [4] 1/(2(a+b)),
+//   [5] c_a c_b exp(-ab/(a+b) r2) / (a+b),  [6] 2a (the ip1 factor of the bra).
+// A quartet builds the rows of its bra and ket pairs once (lanes over pairs),
+// so the per-slot work below has one division and one square root instead of
+// the ~8 divisions and the exponential of the direct evaluation.
+static constexpr int kPairStride = 8;
+// pair rows of one quartet are kept in shared memory up to this many doubles;
+// larger contractions compute the rows of each slot on the fly
+static constexpr int kPairTabMax = 640;
+
+__device__ __forceinline__ void pair_row(const Shell &a, const Shell &b, const PairMask &m, int k,
+                                         const double *__restrict__ R, double r2, double *__restrict__ p)
+{
+    int ia, ib;
+    kept_pair(m, k, ia, ib);
+    const double ea = a.exps[ia], eb = b.exps[ib];
+    const double sab = ea + eb, is = 1.0 / sab;
+    p[0] = -eb * is * R[0];
+    p[1] = -eb * is * R[1];
+    p[2] = -eb * is * R[2];
+    p[3] = sab;
+    p[4] = 0.5 * is;
+    p[5] = a.coefs[ia] * b.coefs[ib] * exp(-ea * eb * is * r2) * is;
+    p[6] = 2.0 * ea;
+    p[7] = 0.0;
+}
+
+// Pair rows of both pairs into tab (bra rows first, then ket rows);
+// threads tid, tid + nt, ... of the cooperating group.
+__device__ __forceinline__ void build_pair_tables(const Shell &si, const Shell &sj, const Shell &sk,
+                                                  const Shell &sl, const PairMask &mb, const PairMask &mk,
+                                                  const double *__restrict__ AB, double rab2,
+                                                  const double *__restrict__ CD, double rcd2,
+                                                  double *__restrict__ tab, int tid, int nt)
+{
+    for (int k = tid; k < mb.n + mk.n; k += nt) {
+        if (k < mb.n)
+            pair_row(si, sj, mb, k, AB, rab2, tab + k * kPairStride);
+        else
+            pair_row(sk, sl, mk, k - mb.n, CD, rcd2, tab + k * kPairStride);
+    }
+}
+
+// ---- slot parameters (phase A, part 2) ----
+// Slots s in [s0, s1) (slot = primitive quartet pq * nroots + root r), one
+// per thread: Rys node/weight r of pq and the recurrence coefficients,
+// written to par[(s - s0) * kParStride + 0..10].  With tab == nullptr the
+// pair rows are computed here (contractions too long for the table).
+__device__ __forceinline__ void slot_params(const double *__restrict__ tab, const Shell &si, const Shell &sj,
+                                            const Shell &sk, const Shell &sl, const PairMask &mb,
+                                            const PairMask &mk, const double *__restrict__ AB, double rab2,
+                                            const double *__restrict__ CD, double rcd2, int nroots, double pref0,
+                                            int s0, int s1, double *__restrict__ par, int tid, int nt)
+{
+    for (int s = s0 + tid; s < s1; s += nt) {
+        const int pq = s / nroots, r = s - pq * nroots;
+        const int ib = pq / mk.n, ik = pq - ib * mk.n;
+        double bl[kPairStride], kl[kPairStride];
+        const double *bp, *kp;
+        if (tab) {
+            bp = tab + ib * kPairStride;
+            kp = tab + (mb.n + ik) * kPairStride;
+        } else {
+            pair_row(si, sj, mb, ib, AB, rab2, bl);
+            pair_row(sk, sl, mk, ik, CD, rcd2, kl);
+            bp = bl;
+            kp = kl;
+        }
+        const double aij = bp[3], akl = kp[3];
+        const double inv = 1.0 / (aij + akl);
+        double PQ[3];
+#pragma unroll
+        for (int x = 0; x < 3; x++) PQ[x] = (si.R[x] + bp[x]) - (sk.R[x] + kp[x]);
+        const double rpq2 = PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2];
+        double u, w;
+        rys_node(nroots, r, aij * akl * inv * rpq2, u, w);
+        double *p = par + (s - s0) * kParStride;
+        const double ua = u * inv;
+#pragma unroll
+        for (int x = 0; x < 3; x++) {
+            p[x] = bp[x] - ua * akl * PQ[x];
+            p[3 + x] = kp[x] + ua * aij * PQ[x];
+        }
+        p[6] = 0.5 * ua;
+        p[7] = bp[4] * (1.0 - ua * akl);
+        p[8] = kp[4] * (1.0 - ua * aij);
+        p[9] = w * pref0 * bp[5] * kp[5] * sqrt(inv);
+        p[10] = bp[6];
+    }
+}
+
 __device__ __forceinline__ double common_fac(int l)
 {
     return l == 0 ? 0.282094791773878143 : (l == 1 ? 0.488602511902919921 : 1.0);
@@ -314,10 +409,6 @@ __device__ void eri_quartet(const int *__restrict__ atm, const int *__restrict__
     const int nf = nfi * nfj * nfk * nfl;
     const int nroots = (li + lj + lk + ll + D) / 2 + 1;
     const int sj = li + 1 + D, sk = sj * (lj + 1), sl = sk * (lk + 1), gsz = sl * (ll + 1);
-    int ns = smem_warp / (3 * gsz + kParStride);
-    ns = ns > kMaxSlots ? kMaxSlots : ns;
-    double *par = wsm;
-    double *gbuf = wsm + ns * kParStride;
     double AB[3], CD[3];
     for (int x = 0; x < 3; x++) {
         AB[x] = si.R[x] - sj_.R[x];
@@ -329,6 +420,15 @@ __device__ void eri_quartet(const int *__restrict__ atm, const int *__restrict__
     const int nslot = mb.n * mk.n * nroots;
     const double pref0 = 34.986836655249725693 * common_fac(li) * common_fac(lj) * common_fac(lk) *
                          common_fac(ll);   // 2 pi^(5/2) x angular factors of s, p
+    // shared memory: [pair rows][slot parameters][2D tables]
+    int tabn = (mb.n + mk.n) * kPairStride;
+    if (tabn > kPairTabMax || smem_warp - tabn < 3 * gsz + kParStride) tabn = 0;
+    int ns = (smem_warp - tabn) / (3 * gsz + kParStride);
+    ns = ns > kMaxSlots ? kMaxSlots : ns;
+    double *tab = tabn ? wsm : nullptr;
+    double *par = wsm + tabn;
+    double *gbuf = par + ns * kParStride;
+    if (tab) build_pair_tables(si, sj_, sk_, sl_, mb, mk, AB, rab2, CD, rcd2, tab, lane, 32);
 
     // Small blocks: the warp splits into NG slot groups of FW lanes (FW >= nf),
     // each group accumulates a strided subset of the slots, and the groups are
@@ -365,42 +465,8 @@ __device__ void eri_quartet(const int *__restrict__ atm, const int *__restrict__
         for (int s0 = 0; s0 < nslot; s0 += ns) {
             const int s1 = min(nslot, s0 + ns);
             __syncwarp();
-            // ---- phase A: primitive-quartet data and Rys nodes/weights
-            const int pq0 = s0 / nroots, pq1 = (s1 - 1) / nroots + 1;
-            for (int pq = pq0 + lane; pq < pq1; pq += 32) {
-                int ip, jp, kp, lp;
-                kept_pair(mb, pq / mk.n, ip, jp);
-                kept_pair(mk, pq % mk.n, kp, lp);
-                const double ai = si.exps[ip], aj = sj_.exps[jp], ak = sk_.exps[kp], al = sl_.exps[lp];
-                const double aij = ai + aj, akl = ak + al, aijkl = aij + akl;
-                double PA[3], QC[3], PQ[3];
-                for (int x = 0; x < 3; x++) {
-                    PA[x] = -aj / aij * AB[x];
-                    QC[x] = -al / akl * CD[x];
-                    PQ[x] = (si.R[x] + PA[x]) - (sk_.R[x] + QC[x]);
-                }
-                const double rpq2 = PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2];
-                const double T = aij * akl / aijkl * rpq2;
-                const double pref = pref0 * si.coefs[ip] * sj_.coefs[jp] * sk_.coefs[kp] * sl_.coefs[lp] *
-                                    exp(-ai * aj / aij * rab2 - ak * al / akl * rcd2) / (aij * akl * sqrt(aijkl));
-                double u[RYS_NROOTS_MAX], w[RYS_NROOTS_MAX];
-                rys_roots(nroots, T, u, w);
-                for (int r = 0; r < nroots; r++) {
-                    const int s = pq * nroots + r;
-                    if (s < s0 || s >= s1) continue;
-                    double *p = par + (s - s0) * kParStride;
-                    const double ua = u[r] / aijkl;
-                    for (int x = 0; x < 3; x++) {
-                        p[x] = PA[x] - ua * akl * PQ[x];
-                        p[3 + x] = QC[x] + ua * aij * PQ[x];
-                    }
-                    p[6] = 0.5 * ua;
-                    p[7] = 0.5 / aij * (1.0 - ua * akl);
-                    p[8] = 0.5 / akl * (1.0 - ua * aij);
-                    p[9] = w[r] * pref;
-                    p[10] = 2.0 * ai;
-                }
-            }
+            // ---- phase A: Rys nodes/weights and recurrence coefficients, one slot per lane
+            slot_params(tab, si, sj_, sk_, sl_, mb, mk, AB, rab2, CD, rcd2, nroots, pref0, s0, s1, par, lane, 32);
             __syncwarp();
             // ---- phase B: recurrences, one (slot, direction) per lane
             for (int it = lane; it < (s1 - s0) * 3; it += 32) {
@@ -749,10 +815,6 @@ __device__ void eri_quartet_hc(const int *__restrict__ atm, const int *__restric
     const int li = si.l, lj = sj_.l, lk = sk_.l, ll = sl_.l;      // computed orientation
     const int le = li + lj + D, lf = lk + ll, s2 = (le + 1) * (lf + 1);
     const int nroots = (li + lj + lk + ll + D) / 2 + 1;
-    int ns = cap / (3 * s2 + kParStride);
-    ns = ns > kMaxSlots ? kMaxSlots : ns;
-    double *par = wsm;
-    double *gbuf = wsm + ns * kParStride;
     double AB[3], CD[3];
     for (int x = 0; x < 3; x++) {
         AB[x] = si.R[x] - sj_.R[x];
@@ -764,6 +826,15 @@ __device__ void eri_quartet_hc(const int *__restrict__ atm, const int *__restric
     const int nslot = mb.n * mk.n * nroots;
     const double pref0 = 34.986836655249725693 * common_fac(li) * common_fac(lj) * common_fac(lk) *
                          common_fac(ll);
+    // shared memory: [pair rows][slot parameters][2D tables]
+    int tabn = (mb.n + mk.n) * kPairStride;
+    if (tabn > (NT == 32 ? kPairTabMax : cap / 4) || cap - tabn < 3 * s2 + kParStride) tabn = 0;
+    int ns = (cap - tabn) / (3 * s2 + kParStride);
+    ns = ns > kMaxSlots ? kMaxSlots : ns;
+    double *tab = tabn ? wsm : nullptr;
+    double *par = wsm + tabn;
+    double *gbuf = par + ns * kParStride;
+    if (tab) build_pair_tables(si, sj_, sk_, sl_, mb, mk, AB, rab2, CD, rcd2, tab, lane, NT);
 
     // lane-owned accumulators: flat t = lane + 32 j = setoff[s] + ie * nf_ket + if
     int idx[NJ];
@@ -791,42 +862,8 @@ __device__ void eri_quartet_hc(const int *__restrict__ atm, const int *__restric
     for (int s0 = 0; s0 < nslot; s0 += ns) {
         const int s1 = min(nslot, s0 + ns);
         grp_sync<NT>();
-        // ---- phase A: primitive-quartet data and Rys nodes/weights (as in eri_quartet)
-        const int pq0 = s0 / nroots, pq1 = (s1 - 1) / nroots + 1;
-        for (int pq = pq0 + lane; pq < pq1; pq += NT) {
-            int ip, jp, kp, lp;
-            kept_pair(mb, pq / mk.n, ip, jp);
-            kept_pair(mk, pq % mk.n, kp, lp);
-            const double ai = si.exps[ip], aj = sj_.exps[jp], ak = sk_.exps[kp], al = sl_.exps[lp];
-            const double aij = ai + aj, akl = ak + al, aijkl = aij + akl;
-            double PA[3], QC[3], PQ[3];
-            for (int x = 0; x < 3; x++) {
-                PA[x] = -aj / aij * AB[x];
-                QC[x] = -al / akl * CD[x];
-                PQ[x] = (si.R[x] + PA[x]) - (sk_.R[x] + QC[x]);
-            }
-            const double rpq2 = PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2];
-            const double T = aij * akl / aijkl * rpq2;
-            const double pref = pref0 * si.coefs[ip] * sj_.coefs[jp] * sk_.coefs[kp] * sl_.coefs[lp] *
-                                exp(-ai * aj / aij * rab2 - ak * al / akl * rcd2) / (aij * akl * sqrt(aijkl));
-            double u[RYS_NROOTS_MAX], w[RYS_NROOTS_MAX];
-            rys_roots(nroots, T, u, w);
-            for (int r = 0; r < nroots; r++) {
-                const int s = pq * nroots + r;
-                if (s < s0 || s >= s1) continue;
-                double *p = par + (s - s0) * kParStride;
-                const double ua = u[r] / aijkl;
-                for (int x = 0; x < 3; x++) {
-                    p[x] = PA[x] - ua * akl * PQ[x];
-                    p[3 + x] = QC[x] + ua * aij * PQ[x];
-                }
-                p[6] = 0.5 * ua;
-                p[7] = 0.5 / aij * (1.0 - ua * akl);
-                p[8] = 0.5 / akl * (1.0 - ua * aij);
-                p[9] = w[r] * pref;
-                p[10] = 2.0 * ai;
-            }
-        }
+        // ---- phase A: Rys nodes/weights and recurrence coefficients, one slot per thread
+        slot_params(tab, si, sj_, sk_, sl_, mb, mk, AB, rab2, CD, rcd2, nroots, pref0, s0, s1, par, lane, NT);
         grp_sync<NT>();
         // ---- phase B: 2D tables, one (slot, direction) per lane
         for (int it = lane; it < (s1 - s0) * 3; it += NT) {
@@ -1050,10 +1087,6 @@ __device__ void eri_quartet_cta(const int *__restrict__ atm, const int *__restri
     const int ne = nf * NC;
     const int nroots = (li + lj + lk + ll + D) / 2 + 1;
     const int sj = li + 1 + D, sk = sj * (lj + 1), sl = sk * (lk + 1), gsz = sl * (ll + 1);
-    int ns = smem_doubles / (3 * gsz + kParStride);
-    ns = ns > kMaxSlots ? kMaxSlots : ns;
-    double *par = sm;
-    double *gbuf = sm + ns * kParStride;
     double AB[3], CD[3];
     for (int x = 0; x < 3; x++) {
         AB[x] = si.R[x] - sj_.R[x];
@@ -1064,6 +1097,15 @@ __device__ void eri_quartet_cta(const int *__restrict__ atm, const int *__restri
     const PairMask mb = pair_mask(si, sj_, rab2, li + lj + D), mk = pair_mask(sk_, sl_, rcd2, lk + ll);
     const int nslot = mb.n * mk.n * nroots;
     const double pref0 = 34.986836655249725693 * common_fac(li) * common_fac(lj) * common_fac(lk) * common_fac(ll);
+    // shared memory: [pair rows][slot parameters][2D tables]
+    int tabn = (mb.n + mk.n) * kPairStride;
+    if (tabn > smem_doubles / 4 || smem_doubles - tabn < 3 * gsz + kParStride) tabn = 0;
+    int ns = (smem_doubles - tabn) / (3 * gsz + kParStride);
+    ns = ns > kMaxSlots ? kMaxSlots : ns;
+    double *tab = tabn ? sm : nullptr;
+    double *par = sm + tabn;
+    double *gbuf = par + ns * kParStride;
+    if (tab) build_pair_tables(si, sj_, sk_, sl_, mb, mk, AB, rab2, CD, rcd2, tab, tid, kHeavyThreads);
     double qv[6] = {0, 0, 0, 0, 0, 0};
 
     for (int e0 = 0; e0 < ne; e0 += kHeavyThreads * kHeavyAcc) {
@@ -1095,41 +1137,8 @@ __device__ void eri_quartet_cta(const int *__restrict__ atm, const int *__restri
         for (int s0 = 0; s0 < nslot; s0 += ns) {
             const int s1 = min(nslot, s0 + ns);
             __syncthreads();
-            const int pq0 = s0 / nroots, pq1 = (s1 - 1) / nroots + 1;
-            for (int pq = pq0 + tid; pq < pq1; pq += kHeavyThreads) {
-                int ip, jp, kp, lp;
-                kept_pair(mb, pq / mk.n, ip, jp);
-                kept_pair(mk, pq % mk.n, kp, lp);
-                const double ai = si.exps[ip], aj = sj_.exps[jp], ak = sk_.exps[kp], al = sl_.exps[lp];
-                const double aij = ai + aj, akl = ak + al, aijkl = aij + akl;
-                double PA[3], QC[3], PQ[3];
-                for (int x = 0; x < 3; x++) {
-                    PA[x] = -aj / aij * AB[x];
-                    QC[x] = -al / akl * CD[x];
-                    PQ[x] = (si.R[x] + PA[x]) - (sk_.R[x] + QC[x]);
-                }
-                const double rpq2 = PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2];
-                const double T = aij * akl / aijkl * rpq2;
-                const double pref = pref0 * si.coefs[ip] * sj_.coefs[jp] * sk_.coefs[kp] * sl_.coefs[lp] *
-                                    exp(-ai * aj / aij * rab2 - ak * al / akl * rcd2) / (aij * akl * sqrt(aijkl));
-                double u[RYS_NROOTS_MAX], w[RYS_NROOTS_MAX];
-                rys_roots(nroots, T, u, w);
-                for (int r = 0; r < nroots; r++) {
-                    const int s = pq * nroots + r;
-                    if (s < s0 || s >= s1) continue;
-                    double *p = par + (s - s0) * kParStride;
-                    const double ua = u[r] / aijkl;
-                    for (int x = 0; x < 3; x++) {
-                        p[x] = PA[x] - ua * akl * PQ[x];
-                        p[3 + x] = QC[x] + ua * aij * PQ[x];
-                    }
-                    p[6] = 0.5 * ua;
-                    p[7] = 0.5 / aij * (1.0 - ua * akl);
-                    p[8] = 0.5 / akl * (1.0 - ua * aij);
-                    p[9] = w[r] * pref;
-                    p[10] = 2.0 * ai;
-                }
-            }
+            slot_params(tab, si, sj_, sk_, sl_, mb, mk, AB, rab2, CD, rcd2, nroots, pref0, s0, s1, par, tid,
+                        kHeavyThreads);
             __syncthreads();
             for (int it = tid; it < (s1 - s0) * 3; it += kHeavyThreads) {
                 const int s = it / 3, dir = it - s * 3;

@@ -58,4 +58,49 @@ static __device__ __noinline__ void rys_roots(int n, double x, double *__restric
     }
 }
 
+// Node r and weight r only (0 <= r < n): the two Chebyshev series run as two
+// interleaved, independent Clenshaw chains.  Used where one lane evaluates one
+// quadrature point of a primitive quartet, so the lanes of a warp split the n
+// points instead of one lane running all 2n series one after the other.
+static __device__ __forceinline__ void rys_node(int n, int r, double x, double &u, double &w)
+{
+    const double xmax = 40.0 + 5.0 * n;
+    if (x < xmax) {
+        const int nint = 16 + 2 * n;
+        int it = (int)(x * RYS_INV_WIDTH);
+        it = it < 0 ? 0 : (it >= nint ? nint - 1 : it);
+        const double t = (x - it * RYS_WIDTH) * (2.0 * RYS_INV_WIDTH) - 1.0;
+        const double t2 = t + t;
+        const double *cu = RYS_CHEB + RYS_CHEB_OFFSET[n - 1] + (it * (2 * n) + r) * (RYS_DEGREE + 1);
+        const double *cw = cu + n * (RYS_DEGREE + 1);
+        double cuv[RYS_DEGREE + 1], cwv[RYS_DEGREE + 1];
+#pragma unroll
+        for (int k = 0; k < (RYS_DEGREE + 1) / 2; k++) {
+            const double2 a = __ldg(reinterpret_cast<const double2 *>(cu) + k);
+            const double2 b = __ldg(reinterpret_cast<const double2 *>(cw) + k);
+            cuv[2 * k] = a.x;
+            cuv[2 * k + 1] = a.y;
+            cwv[2 * k] = b.x;
+            cwv[2 * k + 1] = b.y;
+        }
+        double u1 = 0.0, u2 = 0.0, w1 = 0.0, w2 = 0.0;
+#pragma unroll
+        for (int k = RYS_DEGREE; k >= 1; k--) {
+            const double u0 = fma(t2, u1, cuv[k] - u2);
+            const double w0 = fma(t2, w1, cwv[k] - w2);
+            u2 = u1;
+            u1 = u0;
+            w2 = w1;
+            w1 = w0;
+        }
+        u = fma(t, u1, cuv[0] - u2);
+        w = fma(t, w1, cwv[0] - w2);
+    } else {
+        const int off = n * (n - 1) / 2;
+        const double inv = 1.0 / x;
+        u = RYS_LARGEX_U[off + r] * inv;
+        w = RYS_LARGEX_W[off + r] * sqrt(inv);
+    }
+}
+
 }  // namespace cb
