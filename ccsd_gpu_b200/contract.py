@@ -134,6 +134,8 @@ def mark_constant(*tensors):
     for t in tensors:
         if t is None or not isinstance(t, torch.Tensor) or t.device.type != "cuda":
             continue
+        if torch._C._functorch.is_functorch_wrapped_tensor(t):
+            continue                  # inside torch.func.vmap: no storage to key on
         ptr = t.untyped_storage().data_ptr()
         _const[ptr] = weakref.ref(t, lambda _r, ptr=ptr: _forget(ptr))
 
@@ -273,6 +275,13 @@ def contract(spec, a, b, out=None, alpha=1.0, beta=0.0, mode="tf32x3", stream=No
                 if shape_map.setdefault(ix, n) != n:
                     raise ValueError("size mismatch for index %r in %r" % (ix, spec))
     dev = ta[0][1].device
+    if mode == "fp64" and out is None:
+        # no zero-filled output to copy into: also keeps the FP64 path free of
+        # in-place writes, so it runs under torch.func.vmap (batched solves)
+        STATS["flops"] += 2 * int(np.prod(list(shape_map.values())))
+        STATS["gemms"] += 1
+        res = torch.einsum(spec, _combine(ta), _combine(tb))
+        return res * alpha if alpha != 1.0 else res
     if out is None:
         out = torch.zeros([shape_map[i] for i in so], dtype=torch.float64, device=dev)
         beta = 0.0

@@ -121,7 +121,7 @@ __global__ void c2s_kl_kernel(const double *__restrict__ in, double *__restrict_
 static int smem_per_warp(int lmax, int deriv)
 {
     const int gsz = (lmax + 1 + deriv) * (lmax + 1) * (lmax + 1) * (lmax + 1);
-    int need = 3 * gsz + kParStride;
+    int need = 3 * (gsz | 1) + kParStride;
     if (lmax <= 2 && need < kHcSmem) need = kHcSmem;     // contracted-HRR path
     return need < 2048 ? 2048 : need;
 }
@@ -130,7 +130,7 @@ static int smem_per_warp(int lmax, int deriv)
 static int heavy_smem_doubles(int lmax, int deriv)
 {
     const int gsz = (lmax + 1 + deriv) * (lmax + 1) * (lmax + 1) * (lmax + 1);
-    const long long want = (long long)kMaxSlots * (3 * gsz + kParStride);
+    const long long want = (long long)kMaxSlots * (3 * (gsz | 1) + kParStride);
     const long long cap = 200 * 1024 / 8;
     return (int)(want < cap ? want : cap);
 }

@@ -421,9 +421,12 @@ __device__ void eri_quartet(const int *__restrict__ atm, const int *__restrict__
     const double pref0 = 34.986836655249725693 * common_fac(li) * common_fac(lj) * common_fac(lk) *
                          common_fac(ll);   // 2 pi^(5/2) x angular factors of s, p
     // shared memory: [pair rows][slot parameters][2D tables]
+    // per-direction table stride: odd, so the lanes of phase B (one table
+    // each) and of phase C (different elements of one table) spread over the banks
+    const int gst = gsz | 1;
     int tabn = (mb.n + mk.n) * kPairStride;
-    if (tabn > kPairTabMax || smem_warp - tabn < 3 * gsz + kParStride) tabn = 0;
-    int ns = (smem_warp - tabn) / (3 * gsz + kParStride);
+    if (tabn > kPairTabMax || smem_warp - tabn < 3 * gst + kParStride) tabn = 0;
+    int ns = (smem_warp - tabn) / (3 * gst + kParStride);
     ns = ns > kMaxSlots ? kMaxSlots : ns;
     double *tab = tabn ? wsm : nullptr;
     double *par = wsm + tabn;
@@ -472,12 +475,12 @@ __device__ void eri_quartet(const int *__restrict__ atm, const int *__restrict__
             for (int it = lane; it < (s1 - s0) * 3; it += 32) {
                 const int s = it / 3, dir = it - s * 3;
                 build_g_any<D, LOW>(par + s * kParStride, dir, li, lj, lk, ll, AB[dir], CD[dir],
-                               gbuf + (s * 3 + dir) * gsz);
+                               gbuf + (s * 3 + dir) * gst);
             }
             __syncwarp();
             // ---- phase C: accumulate
             for (int s = grp; s < s1 - s0; s += NG) {
-                const double *gx = gbuf + s * 3 * gsz, *gy = gx + gsz, *gz = gy + gsz;
+                const double *gx = gbuf + s * 3 * gst, *gy = gx + gst, *gz = gy + gst;
                 const double ai2 = par[s * kParStride + 10];
 #pragma unroll
                 for (int n = 0; n < GW; n++) {
@@ -827,9 +830,10 @@ __device__ void eri_quartet_hc(const int *__restrict__ atm, const int *__restric
     const double pref0 = 34.986836655249725693 * common_fac(li) * common_fac(lj) * common_fac(lk) *
                          common_fac(ll);
     // shared memory: [pair rows][slot parameters][2D tables]
+    const int s2t = s2 | 1;     // odd per-direction table stride (bank spread)
     int tabn = (mb.n + mk.n) * kPairStride;
-    if (tabn > (NT == 32 ? kPairTabMax : cap / 4) || cap - tabn < 3 * s2 + kParStride) tabn = 0;
-    int ns = (cap - tabn) / (3 * s2 + kParStride);
+    if (tabn > (NT == 32 ? kPairTabMax : cap / 4) || cap - tabn < 3 * s2t + kParStride) tabn = 0;
+    int ns = (cap - tabn) / (3 * s2t + kParStride);
     ns = ns > kMaxSlots ? kMaxSlots : ns;
     double *tab = tabn ? wsm : nullptr;
     double *par = wsm + tabn;
@@ -868,12 +872,12 @@ __device__ void eri_quartet_hc(const int *__restrict__ atm, const int *__restric
         // ---- phase B: 2D tables, one (slot, direction) per lane
         for (int it = lane; it < (s1 - s0) * 3; it += NT) {
             const int s = it / 3, dir = it - s * 3;
-            hc_build_any(par + s * kParStride, dir, le, lf, gbuf + (s * 3 + dir) * s2);
+            hc_build_any(par + s * kParStride, dir, le, lf, gbuf + (s * 3 + dir) * s2t);
         }
         grp_sync<NT>();
         // ---- phase C: [e|f] += Ix Iy Iz (x 2 a_i on the raised set)
         for (int s = 0; s < s1 - s0; s++) {
-            const double *gx = gbuf + s * 3 * s2, *gy = gx + s2, *gz = gy + s2;
+            const double *gx = gbuf + s * 3 * s2t, *gy = gx + s2t, *gz = gy + s2t;
             const double a2 = par[s * kParStride + 10];
 #pragma unroll
             for (int j = 0; j < NJ; j++) {
@@ -1098,9 +1102,10 @@ __device__ void eri_quartet_cta(const int *__restrict__ atm, const int *__restri
     const int nslot = mb.n * mk.n * nroots;
     const double pref0 = 34.986836655249725693 * common_fac(li) * common_fac(lj) * common_fac(lk) * common_fac(ll);
     // shared memory: [pair rows][slot parameters][2D tables]
+    const int gst = gsz | 1;     // odd per-direction table stride (bank spread)
     int tabn = (mb.n + mk.n) * kPairStride;
-    if (tabn > smem_doubles / 4 || smem_doubles - tabn < 3 * gsz + kParStride) tabn = 0;
-    int ns = (smem_doubles - tabn) / (3 * gsz + kParStride);
+    if (tabn > smem_doubles / 4 || smem_doubles - tabn < 3 * gst + kParStride) tabn = 0;
+    int ns = (smem_doubles - tabn) / (3 * gst + kParStride);
     ns = ns > kMaxSlots ? kMaxSlots : ns;
     double *tab = tabn ? sm : nullptr;
     double *par = sm + tabn;
@@ -1143,11 +1148,11 @@ __device__ void eri_quartet_cta(const int *__restrict__ atm, const int *__restri
             for (int it = tid; it < (s1 - s0) * 3; it += kHeavyThreads) {
                 const int s = it / 3, dir = it - s * 3;
                 build_g_any<D, LOW>(par + s * kParStride, dir, li, lj, lk, ll, AB[dir], CD[dir],
-                                    gbuf + (s * 3 + dir) * gsz);
+                                    gbuf + (s * 3 + dir) * gst);
             }
             __syncthreads();
             for (int s = 0; s < s1 - s0; s++) {
-                const double *gx = gbuf + s * 3 * gsz, *gy = gx + gsz, *gz = gy + gsz;
+                const double *gx = gbuf + s * 3 * gst, *gy = gx + gst, *gz = gy + gst;
                 const double ai2 = par[s * kParStride + 10];
 #pragma unroll
                 for (int n = 0; n < kHeavyAcc; n++) {

@@ -9,7 +9,7 @@ namespace cb {
 static constexpr int kWarps = 4;          // warps (quartets in flight) per CTA of the warp kernels
 static constexpr int kHeavyThreads = 256; // threads of the CTA (heavy-quartet) kernels
 static constexpr int kMaxSlots = 64;      // slots per batch cap
-static constexpr int kParStride = 12;     // doubles of per-slot parameters
+static constexpr int kParStride = 13;     // doubles of per-slot parameters (odd: lanes spread over banks)
 static constexpr int kHcSmem = 3072;      // doubles of shared memory per warp on the contracted-HRR path
 
 // Quartets whose Cartesian block has more functions than heavy_nf(D) go to

@@ -61,6 +61,29 @@ def lclass(bas, q):
     return np.maximum(a, b) * 100 + np.minimum(a, b)
 
 
+def candidate_quartets(nb, m, rng):
+    """m uniformly drawn unique-order quartets (i>=j, k>=l, ij>=kl) of nb shells."""
+    i = rng.integers(0, nb, m)
+    j = rng.integers(0, nb, m)
+    k = rng.integers(0, nb, m)
+    l = rng.integers(0, nb, m)
+    ij = np.stack([np.maximum(i, j), np.minimum(i, j)], 1)
+    kl = np.stack([np.maximum(k, l), np.minimum(k, l)], 1)
+    pij = ij[:, 0].astype(np.int64) * (ij[:, 0] + 1) // 2 + ij[:, 1]
+    pkl = kl[:, 0].astype(np.int64) * (kl[:, 0] + 1) // 2 + kl[:, 1]
+    swap = pkl > pij
+    a = np.where(swap[:, None], kl, ij)
+    b = np.where(swap[:, None], ij, kl)
+    return np.concatenate([a, b], 1).astype(np.int32)
+
+
+def first_candidate_chunk(shells, n, seed=1, oversample=4):
+    """The first candidate chunk :func:`sample_quartets` draws for a sample of
+    n: screening a prefix of it yields quartets that are a prefix, in draw
+    order, of the same sample (a uniform subset of it)."""
+    return candidate_quartets(shells.nbas, n * oversample + 1024, np.random.default_rng(seed))
+
+
 def sample_quartets(shells, n, seed=1, schwarz_fn=None, threshold=1e-12, oversample=4):
     """Uniform sample of unique quartets (i>=j, k>=l, ij>=kl) passing the screen.
 
@@ -73,18 +96,7 @@ def sample_quartets(shells, n, seed=1, schwarz_fn=None, threshold=1e-12, oversam
     have = 0
     while have < n:
         m = (n - have) * oversample + 1024
-        i = rng.integers(0, nb, m)
-        j = rng.integers(0, nb, m)
-        k = rng.integers(0, nb, m)
-        l = rng.integers(0, nb, m)
-        ij = np.stack([np.maximum(i, j), np.minimum(i, j)], 1)
-        kl = np.stack([np.maximum(k, l), np.minimum(k, l)], 1)
-        pij = ij[:, 0].astype(np.int64) * (ij[:, 0] + 1) // 2 + ij[:, 1]
-        pkl = kl[:, 0].astype(np.int64) * (kl[:, 0] + 1) // 2 + kl[:, 1]
-        swap = pkl > pij
-        a = np.where(swap[:, None], kl, ij)
-        b = np.where(swap[:, None], ij, kl)
-        q = np.concatenate([a, b], 1).astype(np.int32)
+        q = candidate_quartets(nb, m, rng)
         if schwarz_fn is not None:
             pairs = np.concatenate([q[:, :2], q[:, 2:]], 0)
             keys = pairs[:, 0].astype(np.int64) * nb + pairs[:, 1]
