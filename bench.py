@@ -57,7 +57,8 @@ NSHELL = 4096
 
 def parse():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", choices=["eri", "lambda", "gemm", "grad", "autograd", "clusters"], default="eri")
+    ap.add_argument("--workload", choices=["eri", "lambda", "gemm", "grad", "autograd", "clusters", "refgpu"],
+                    default="eri")
     ap.add_argument("--molecules", type=int, default=64, help="clusters workload: molecules per pass (64 = full set)")
     ap.add_argument("--serial-molecules", action="store_true",
                     help="gradient of one molecule after another instead of shape-batched solves")
@@ -84,7 +85,7 @@ def parse():
     ap.add_argument("--no-tune", action="store_true", help="ERI workload: compiled heavy-quartet thresholds")
     args = ap.parse_args()
     dflt = {"eri": (10, 3), "lambda": (3, 3), "gemm": (10, 3), "grad": (5, 3), "autograd": (3, 3),
-            "clusters": (1, 1)}[args.workload]     # clusters: one warm-up pass fills the basis caches
+            "clusters": (1, 1), "refgpu": (2, 1)}[args.workload]     # clusters: one warm-up pass fills the basis caches
     args.steps = dflt[0] if args.steps is None else args.steps
     args.warmup = dflt[1] if args.warmup is None else args.warmup
     return args
@@ -504,6 +505,91 @@ def run_grad(args, ws, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_refgpu(args, ws, rank, local):
+    """Reference-GPU comparator: int2e_ip1 (and int2e) Cartesian s2kl blocks of
+    every atom's shells, as the reference's gradient loop requests them
+    (ref: ccsd_gpu/gpu_ccsd_grad.py:449-457), from the package's kernels and from
+    the reference's own kernels built for sm_100a and launched by its launch loop
+    (oracle/_ref/libref_eri_gpu.so; a baseline leg, never the product path).
+    Also times the package's fused ip1-Gamma gradient contraction of the whole
+    molecule, which replaces the blocks in the package's gradient."""
+    from oracle import ref_gpu
+    from ccsd_gpu_b200 import compute_int2e_gpu, compute_int2e_ip1_gpu, workloads
+    from ccsd_gpu_b200.cuda.ip1_contract import contract_int2e_ip1
+    from ccsd_gpu_b200.gto import M
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if not ref_gpu.available():
+        if rank == 0:
+            print(json.dumps({"workload": "refgpu", "unavailable": "oracle/_ref/libref_eri_gpu.so not built"}))
+        return
+    barrier = (lambda: (torch.distributed.barrier(), torch.cuda.synchronize(dev))) if ws > 1 else \
+        (lambda: torch.cuda.synchronize(dev))
+    sym, xyz = workloads.ethanol_atoms(seed=0)
+    mols = {"h2o": "O 0 0 0; H 0 0.757 0.587; H 0 -0.757 0.587",
+            "ethanol": workloads.atom_string(sym, xyz)}
+    rng = np.random.default_rng(0)
+    for n in (6,):
+        s6, x6 = workloads.water_cluster_atoms(n, rng)
+        mols["h2o_6"] = workloads.atom_string(s6, x6)
+    out = {}
+    steps = max(1, min(args.steps, 3))
+    for name, atom in mols.items():
+        mol = M(atom=atom, basis="cc-pvdz", cart=True)
+        rb = ref_gpu.RefBasis(mol, dev)
+        blocks = [(int(r[0]), int(r[1])) for r in mol.offset_nr_by_atom()]
+        res = {"nao_cart": int(mol.nao_nr()), "atom_blocks": len(blocks)}
+        for deriv in (1, 0):
+            fn = compute_int2e_ip1_gpu if deriv else compute_int2e_gpu
+            worst = 0.0
+            for b0, b1 in blocks:       # parity (and warm-up) on every block
+                ref = ref_gpu.eri_cart(rb, b0, b1, deriv)
+                got = fn(mol, b0, b1)
+                err = float((got - ref).abs().max() / (ref.abs().max() + 1e-300))
+                worst = max(worst, err)
+                del ref, got
+            torch.cuda.empty_cache()
+
+            def run_ref():
+                for b0, b1 in blocks:
+                    ref_gpu.eri_cart(rb, b0, b1, deriv)
+
+            def run_ours():
+                for b0, b1 in blocks:
+                    fn(mol, b0, b1)
+            with ClockSampler(dev) as clk:
+                kr, _ = _events_timed(run_ref, steps, barrier)
+                ko, _ = _events_timed(run_ours, steps, barrier)
+            tr, to = _maxr(float(kr.mean()), ws, dev), _maxr(float(ko.mean()), ws, dev)
+            res["ip1" if deriv else "int2e"] = {
+                "reference_kernels_ms": tr, "package_kernels_ms": to, "speedup": tr / to,
+                "max_rel_diff_vs_reference_kernels": worst, "clocks": clk.summary()}
+        msph = M(atom=atom, basis="cc-pvdz")
+        nao = msph.nao_nr()
+        g = torch.randn((nao,) * 4, dtype=torch.float64, device=dev, generator=torch.Generator(dev).manual_seed(0))
+        g = g + g.transpose(2, 3)
+        contract_int2e_ip1(msph, g)
+        kf, _ = _events_timed(lambda: contract_int2e_ip1(msph, g), steps, barrier)
+        res["fused_ip1_gamma_ms"] = _maxr(float(kf.mean()), ws, dev)
+        res["fused_speedup_vs_reference_ip1_blocks"] = res["ip1"]["reference_kernels_ms"] / res["fused_ip1_gamma_ms"]
+        del g
+        torch.cuda.empty_cache()
+        out[name] = res
+    big = out["h2o_6"]["ip1"]
+    line = {"metric": "int2e_ip1 atom-block time, reference's kernels / package's kernels on the same B200",
+            "value": big["speedup"], "unit": "x", "n_gpus": ws, "steps": steps, "warmup": 1,
+            "ms_per_step": big["package_kernels_ms"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic geometries",
+            "config": {"workload": "eri_atom_blocks_refgpu", "basis": "cc-pvdz (Cartesian blocks)",
+                       "value_of": "(H2O)6 int2e_ip1",
+                       "reference_launch": "one launch per decontracted i-shell, dim3(1, 32) blocks, as "
+                                           "ccsd_gpu/cuda/int2e_ip1_gpu.py:148-216",
+                       "parallelism": "dp%d" % ws if ws > 1 else "single"},
+            "molecules": out, "roofline": None, "cpu_baseline": None, "e2e": None}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def _ccsd_energy(mol, mode):
     from ccsd_gpu_b200.ccsd import CCSD
     from ccsd_gpu_b200.scf import RHF
@@ -647,7 +733,7 @@ def main():
         return
     if args.workload != "eri":
         {"gemm": run_gemm, "lambda": run_lambda, "grad": run_grad, "autograd": run_autograd,
-         "clusters": run_clusters}[args.workload](args, ws, rank, local)
+         "clusters": run_clusters, "refgpu": run_refgpu}[args.workload](args, ws, rank, local)
         if ws > 1:
             torch.distributed.destroy_process_group()
         return

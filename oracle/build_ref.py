@@ -7,7 +7,9 @@ there is no default location.  It imports the reference's kernel-source modules
 stand-in for ``cupy`` (only ``_build_cuda_source`` and the Rys data loader are
 called, no CuPy object is touched), writes the generated kernel source to
 oracle/_ref/*.inc and compiles oracle/ref_eri_shim.cpp against it with g++ and
-OpenMP into oracle/_ref/libref_eri.so.  Nothing here is copied into the
+OpenMP into oracle/_ref/libref_eri.so, and oracle/ref_eri_gpu.cu with nvcc for
+sm_100a into oracle/_ref/libref_eri_gpu.so (the reference's kernels on the
+GPU, as a comparator).  Nothing here is copied into the
 repository: oracle/_ref/ is git-ignored and only travels with the working
 tree.
 """
@@ -70,6 +72,25 @@ def build(ref_root=None, verbose=False):
     so = os.path.join(OUT, "libref_eri.so")
     cmd = ["g++", "-O2", "-fopenmp", "-fPIC", "-shared", "-std=c++17", "-w",
            "-I", OUT, os.path.join(HERE, "ref_eri_shim.cpp"), "-o", so]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.check_call(cmd)
+    build_gpu(verbose=verbose)
+    return so
+
+
+def build_gpu(verbose=False):
+    """Build oracle/_ref/libref_eri_gpu.so (oracle/ref_eri_gpu.cu: the
+    reference's kernels for sm_100a behind a launcher of the reference's launch
+    loop) from the kernel sources already generated into oracle/_ref/.
+    Returns None when the sources or nvcc are missing."""
+    import shutil
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not (os.path.exists(os.path.join(OUT, "int2e_src.inc")) and os.path.exists(nvcc)):
+        return None
+    so = os.path.join(OUT, "libref_eri_gpu.so")
+    cmd = [nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
+           "-shared", "-w", "-I", OUT, os.path.join(HERE, "ref_eri_gpu.cu"), "-o", so]
     if verbose:
         print(" ".join(cmd))
     subprocess.check_call(cmd)
