@@ -36,6 +36,8 @@ SIGNATURES = {
     "ccsd_b200_eri_full_cart": (_c_int, [_vp, _vp, _vp, _vp, _c_int, _vp, _c_ll, _c_int, _vp, _vp]),
     "ccsd_b200_eri_ip1_contract": (_c_int, [_vp, _vp, _vp, _vp, _c_int, _vp, _vp, _c_ll, _vp, _c_int, _c_int, _vp,
                                             _vp, _vp]),
+    "ccsd_b200_eri_ip1_contract_rows": (_c_int, [_vp, _vp, _vp, _vp, _c_int, _vp, _c_int, _c_int, _vp, _c_ll, _vp,
+                                                 _c_int, _c_int, _vp, _vp, _vp]),
     "ccsd_b200_wait_probe": (_c_int, [_vp, _c_ll, _c_int, _vp]),
     "ccsd_b200_tc_split_gemm": (_c_int, [_c_int, _vp, _vp, _vp, _vp, _c_int, _c_int, _c_int, _c_int, _c_int,
                                          _vp, _vp, _vp, _c_dbl, _c_dbl, _c_int, _vp, _vp, _vp]),

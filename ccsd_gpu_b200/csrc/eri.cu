@@ -329,12 +329,13 @@ int ccsd_b200_eri_quartet_checksums(int deriv, const int32_t *atm, const int32_t
     return run_pair(Kind::QSUM, deriv, lmax <= 2, a, nq, nq, (cudaStream_t)stream);
 }
 
-int ccsd_b200_eri_ip1_contract(const int32_t *atm, const int32_t *bas, const double *env, const int32_t *ao_loc,
-                               int nao, const double *gamma, const int32_t *quartets, long long nq,
-                               const long long *seg, int nseg, int lmax, double *qwork, double *out, void *stream)
+int ccsd_b200_eri_ip1_contract_rows(const int32_t *atm, const int32_t *bas, const double *env,
+                                    const int32_t *ao_loc, int nao, const double *gamma_rows, int row0, int nrows,
+                                    const int32_t *quartets, long long nq, const long long *seg, int nseg, int lmax,
+                                    double *qwork, double *out, void *stream)
 {
-    if (!atm || !bas || !env || !ao_loc || nao <= 0 || !gamma || !quartets || nq < 0 || !seg || nseg <= 0 ||
-        lmax < 0 || !qwork || !out) {
+    if (!atm || !bas || !env || !ao_loc || nao <= 0 || !gamma_rows || row0 < 0 || nrows <= 0 || row0 + nrows > nao ||
+        !quartets || nq < 0 || !seg || nseg <= 0 || lmax < 0 || !qwork || !out) {
         set_error("ccsd_b200_eri_ip1_contract: invalid argument");
         return CCSD_B200_ERR_ARG;
     }
@@ -351,7 +352,9 @@ int ccsd_b200_eri_ip1_contract(const int32_t *atm, const int32_t *bas, const dou
         a.env = env;
         a.ao_loc = ao_loc;
         a.nao = nao;
-        a.gamma = gamma;
+        a.gamma = gamma_rows;
+        a.grow0 = row0;
+        a.grows = nrows;
         a.quartets = reinterpret_cast<const int4 *>(quartets);
         a.nq = nq;
         a.qsum = qwork;
@@ -362,6 +365,14 @@ int ccsd_b200_eri_ip1_contract(const int32_t *atm, const int32_t *bas, const dou
     }
     segment_sum3_kernel<<<nseg, 256, 0, st>>>(qwork, seg, out);
     return check_launch("segment_sum3_kernel");
+}
+
+int ccsd_b200_eri_ip1_contract(const int32_t *atm, const int32_t *bas, const double *env, const int32_t *ao_loc,
+                               int nao, const double *gamma, const int32_t *quartets, long long nq,
+                               const long long *seg, int nseg, int lmax, double *qwork, double *out, void *stream)
+{
+    return ccsd_b200_eri_ip1_contract_rows(atm, bas, env, ao_loc, nao, gamma, 0, nao, quartets, nq, seg, nseg, lmax,
+                                           qwork, out, stream);
 }
 
 int ccsd_b200_eri_full_cart(const int32_t *atm, const int32_t *bas, const double *env, const int32_t *ao_loc,

@@ -150,9 +150,16 @@ __device__ __forceinline__ void kept_pair(const PairMask &m, int k, int &ia, int
 // so the per-slot work below has one division and one square root instead of
 // the ~8 divisions and the exponential of the direct evaluation.
 static constexpr int kPairStride = 8;
-// pair rows of one quartet are kept in shared memory up to this many doubles;
-// larger contractions compute the rows of each slot on the fly
-static constexpr int kPairTabMax = 640;
+// The pair rows of a quartet are kept in shared memory when, beside them, a
+// batch of at least min(nslot, 32) slots still fits (per_slot doubles each);
+// otherwise each slot computes its two rows on the fly (two exponentials and
+// divisions per slot).  Long general contractions (9 x 9 primitive pairs of
+// an oxygen s shell in cc-pVDZ: 1296 doubles) keep their table this way.
+__device__ __forceinline__ bool pair_table_fits(int tabn, int room, int per_slot, int nslot)
+{
+    const int batch = nslot < 32 ? (nslot > 1 ? nslot : 1) : 32;
+    return tabn <= room - batch * per_slot;
+}
 
 __device__ __forceinline__ void pair_row(const Shell &a, const Shell &b, const PairMask &m, int k,
                                          const double *__restrict__ R, double r2, double *__restrict__ p)
@@ -385,7 +392,19 @@ struct S2klOut {
     double *out;
     long long nao_pair, comp_stride;
     int nao, i_base;
-    const double *gamma;     // MODE_GRAD: dense [nao]^4 density in the Cartesian AO basis
+    // MODE_GRAD: rows [g_row0, g_row0 + g_rows) of the dense [nao]^4 density in
+    // the Cartesian AO basis (all rows: g_row0 = 0, g_rows = nao)
+    const double *gamma;
+    int g_row0, g_rows;
+
+    // gamma[i][j][k][l]; 0 for a first index outside the rows held
+    __device__ __forceinline__ double gamma_at(long long i, long long j, long long k, long long l) const
+    {
+        const long long r = i - g_row0;
+        if (r < 0 || r >= g_rows) return 0.0;
+        const long long n = nao;
+        return gamma[((r * n + j) * n + k) * n + l];
+    }
 };
 
 // Integrals of one shell quartet by one warp.  MODE_S2KL writes the s2kl block,
@@ -425,7 +444,7 @@ __device__ void eri_quartet(const int *__restrict__ atm, const int *__restrict__
     // each) and of phase C (different elements of one table) spread over the banks
     const int gst = gsz | 1;
     int tabn = (mb.n + mk.n) * kPairStride;
-    if (tabn > kPairTabMax || smem_warp - tabn < 3 * gst + kParStride) tabn = 0;
+    if (!pair_table_fits(tabn, smem_warp, 3 * gst + kParStride, nslot)) tabn = 0;
     int ns = (smem_warp - tabn) / (3 * gst + kParStride);
     ns = ns > kMaxSlots ? kMaxSlots : ns;
     double *tab = tabn ? wsm : nullptr;
@@ -560,7 +579,7 @@ __device__ void eri_quartet(const int *__restrict__ atm, const int *__restrict__
                     const int fk = t % nfk; t /= nfk;
                     const int fj = t % nfj;
                     const int fi = t / nfj;
-                    const double gv = so.gamma[(((i0 + fi) * nao + (j0 + fj)) * nao + (k0 + fk)) * nao + (l0 + fl)];
+                    const double gv = so.gamma_at(i0 + fi, j0 + fj, k0 + fk, l0 + fl);
 #pragma unroll
                     for (int c = 0; c < NC; c++) sv[c] = fma(acc[n][c], gv, sv[c]);
                 }
@@ -832,7 +851,7 @@ __device__ void eri_quartet_hc(const int *__restrict__ atm, const int *__restric
     // shared memory: [pair rows][slot parameters][2D tables]
     const int s2t = s2 | 1;     // odd per-direction table stride (bank spread)
     int tabn = (mb.n + mk.n) * kPairStride;
-    if (tabn > (NT == 32 ? kPairTabMax : cap / 4) || cap - tabn < 3 * s2t + kParStride) tabn = 0;
+    if (!pair_table_fits(tabn, cap, 3 * s2t + kParStride, nslot)) tabn = 0;
     int ns = (cap - tabn) / (3 * s2t + kParStride);
     ns = ns > kMaxSlots ? kMaxSlots : ns;
     double *tab = tabn ? wsm : nullptr;
@@ -954,7 +973,7 @@ __device__ void eri_quartet_hc(const int *__restrict__ atm, const int *__restric
         } else if (MODE == MODE_GRAD) {
             const long long nao = so.nao;
             const int i0 = ao_loc[ish], j0 = ao_loc[jsh], k0 = ao_loc[ksh], l0 = ao_loc[lsh];
-            const double gv = so.gamma[(((i0 + oi) * nao + (j0 + oj)) * nao + (k0 + fk)) * nao + (l0 + fl)];
+            const double gv = so.gamma_at(i0 + oi, j0 + oj, k0 + fk, l0 + fl);
 #pragma unroll
             for (int c = 0; c < NC; c++) r1[c] = fma(v[c], gv, r1[c]);
         } else {
@@ -1222,8 +1241,7 @@ __device__ void eri_quartet_cta(const int *__restrict__ atm, const int *__restri
                     const int fk = t % nfk; t /= nfk;
                     const int fj = t % nfj;
                     const int fi = t / nfj;
-                    qv[c] = fma(acc[n], so.gamma[(((i0 + fi) * nao + (j0 + fj)) * nao + (k0 + fk)) * nao + (l0 + fl)],
-                                qv[c]);
+                    qv[c] = fma(acc[n], so.gamma_at(i0 + fi, j0 + fj, k0 + fk, l0 + fl), qv[c]);
                 }
             }
         } else {
@@ -1303,7 +1321,7 @@ __global__ void __launch_bounds__(kWarps * 32, 2) eri_qsum_kernel(
     const int *__restrict__ atm, const int *__restrict__ bas, const double *__restrict__ env,
     const int4 *__restrict__ quartets, long long nq, double *__restrict__ qsum, int smem_warp,
     const int *__restrict__ ao_loc = nullptr, const double *__restrict__ gamma = nullptr, int nao = 0,
-    double *__restrict__ full = nullptr, int heavy = 0)
+    double *__restrict__ full = nullptr, int heavy = 0, int grow0 = 0, int grows = 0)
 {
     if (heavy <= 0) heavy = heavy_nf(D);
     extern __shared__ double smem[];
@@ -1311,6 +1329,8 @@ __global__ void __launch_bounds__(kWarps * 32, 2) eri_qsum_kernel(
     double *wsm = smem + warp * smem_warp;
     S2klOut so = {};
     so.gamma = gamma;
+    so.g_row0 = grow0;
+    so.g_rows = grows > 0 ? grows : nao;
     so.out = full;                 // MODE_FULL output
     so.nao = nao;
     constexpr int NC = D ? 3 : 1;
@@ -1373,12 +1393,14 @@ __global__ void __launch_bounds__(kHeavyThreads, 1) eri_qsum_heavy_kernel(
     const int *__restrict__ atm, const int *__restrict__ bas, const double *__restrict__ env,
     const int4 *__restrict__ quartets, long long nq, double *__restrict__ qsum, int smem_doubles,
     const int *__restrict__ ao_loc = nullptr, const double *__restrict__ gamma = nullptr, int nao = 0,
-    double *__restrict__ full = nullptr, int heavy = 0)
+    double *__restrict__ full = nullptr, int heavy = 0, int grow0 = 0, int grows = 0)
 {
     if (heavy <= 0) heavy = heavy_nf(D);
     extern __shared__ double smem[];
     S2klOut so = {};
     so.gamma = gamma;
+    so.g_row0 = grow0;
+    so.g_rows = grows > 0 ? grows : nao;
     so.out = full;                 // MODE_FULL output
     so.nao = nao;
     constexpr int NC = D ? 3 : 1;
@@ -1442,7 +1464,7 @@ int launch_list(const EriArgs &a, long long grid, size_t smem, cudaStream_t st)
     if ((rc = prepare_kernel(eri_qsum_kernel<D, LOW, MODE>, smem))) return rc;
     eri_qsum_kernel<D, LOW, MODE><<<(int)grid, kWarps * 32, smem, st>>>(a.atm, a.bas, a.env, a.quartets, a.nq,
                                                                         a.qsum, a.smem_warp, a.ao_loc, a.gamma,
-                                                                        a.nao, a.full, a.heavy);
+                                                                        a.nao, a.full, a.heavy, a.grow0, a.grows);
     return check_launch("eri_qsum_kernel");
 }
 
@@ -1452,7 +1474,8 @@ int launch_list_heavy(const EriArgs &a, long long grid, size_t smem, cudaStream_
     int rc;
     if ((rc = prepare_kernel(eri_qsum_heavy_kernel<D, LOW, MODE>, smem))) return rc;
     eri_qsum_heavy_kernel<D, LOW, MODE><<<(int)grid, kHeavyThreads, smem, st>>>(
-        a.atm, a.bas, a.env, a.quartets, a.nq, a.qsum, a.smem_heavy, a.ao_loc, a.gamma, a.nao, a.full, a.heavy);
+        a.atm, a.bas, a.env, a.quartets, a.nq, a.qsum, a.smem_heavy, a.ao_loc, a.gamma, a.nao, a.full, a.heavy,
+        a.grow0, a.grows);
     return check_launch("eri_qsum_heavy_kernel");
 }
 

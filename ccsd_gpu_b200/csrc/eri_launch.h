@@ -32,6 +32,7 @@ struct EriArgs {
     long long nq = 0;
     double *qsum = nullptr;                        // per-quartet checksums / gradient values
     const double *gamma = nullptr;                 // MODE_GRAD density
+    int grow0 = 0, grows = 0;                      // MODE_GRAD: rows of gamma held (grows 0: all nao)
     double *full = nullptr;                        // MODE_FULL dense tensor
     int heavy = 0;                                 // heavy-quartet threshold (0: compiled default)
     int smem_warp = 0, smem_heavy = 0;             // doubles of shared memory per warp / per heavy CTA

@@ -97,3 +97,51 @@ def contract_int2e_ip1(mol, gamma, stream=None):
                  _native.ptr(topo.ao_loc_dev), naoc, _native.ptr(gc), _native.ptr(q), nq, _native.ptr(seg),
                  mol.natm, topo.lmax, _native.ptr(qwork), _native.ptr(out), _native.stream(stream))
     return out
+
+
+def contract_int2e_ip1_rows(mol, rows, atom, stream=None):
+    """(3,) FP64 tensor: sum_{i on atom, j, k, l} (d/dx_i ij|kl) gamma[ijkl] from
+    only the atom's rows of gamma.
+
+    ``rows``: (nrows, nao, nao, nao) FP64 on the GPU, the rows
+    ``mol.offset_nr_by_atom()[atom][2:4]`` of gamma in the molecule's AO
+    basis (symmetric in k <-> l).  The rows go to the Cartesian basis of the
+    decontracted shells (the atom's rows only), and the atom's segment of the
+    gradient quartet list is contracted with them by
+    ``ccsd_b200_eri_ip1_contract_rows``.  Summed over atoms this equals
+    :func:`contract_int2e_ip1` of the whole gamma, which never has to exist.
+    """
+    _native.require_cuda(rows)
+    if not _check_mol(mol):
+        raise ValueError("shells with l > 4 are not supported (nroots > 9)")
+    dev = rows.device
+    topo = get_basis_cached(mol, dev)
+    naoc = topo.nao_cart
+    s0, s1, p0, p1 = (int(x) for x in mol.offset_nr_by_atom()[atom])
+    out = torch.zeros(3, dtype=torch.float64, device=dev)
+    if s1 <= s0:
+        return out
+    d0, d1 = topo.orig2dc[s0][0], topo.orig2dc[s1 - 1][-1] + 1
+    c0, c1 = int(topo.dc_ao_loc[d0]), int(topo.dc_ao_loc[d1])
+    if tuple(rows.shape) != (p1 - p0,) + (mol.nao_nr(),) * 3:
+        raise ValueError("rows has shape %s, expected (%d,) + (%d,)*3" % (tuple(rows.shape), p1 - p0, mol.nao_nr()))
+    rows = rows.to(torch.float64)
+    if not mol.cart:
+        from ..lowmem import transform_rows
+        T = torch.as_tensor(topo.sph()["C"], dtype=torch.float64, device=dev)      # (ncart, nsph)
+        rows = transform_rows(rows.contiguous(), T[c0:c1, p0:p1].T, T.T, T.T, T.T).contiguous()
+    atm, env = upload_geometry(mol, dev)
+    q, seg = gradient_quartets(topo, mol.natm)
+    segh = seg.cpu().numpy()
+    qa = q[int(segh[atom]):int(segh[atom + 1])]
+    nq = int(qa.shape[0])
+    if nq:
+        ds = SimpleNamespace(atm=atm, bas=topo.bas_dev, env=env, lmax=topo.lmax)
+        tune.tune_eri_heavy(ds, topo.dc_bas, q, 1, tune.basis_dshare(topo.dc_bas))
+    qwork = torch.empty((max(nq, 1), 3), dtype=torch.float64, device=dev)
+    seg1 = torch.tensor([0, nq], dtype=torch.int64, device=dev)
+    _native.call("ccsd_b200_eri_ip1_contract_rows", _native.ptr(atm), _native.ptr(topo.bas_dev), _native.ptr(env),
+                 _native.ptr(topo.ao_loc_dev), naoc, _native.ptr(rows), c0, c1 - c0, _native.ptr(qa), nq,
+                 _native.ptr(seg1), 1, topo.lmax, _native.ptr(qwork), _native.ptr(out.view(1, 3)),
+                 _native.stream(stream))
+    return out

@@ -170,6 +170,21 @@ int ccsd_b200_eri_ip1_contract(const int32_t *atm, const int32_t *bas, const dou
                                const long long *seg, int nseg, int lmax, double *qwork, double *out, void *stream);
 
 /*
+ * The same contraction with only rows [row0, row0 + nrows) of gamma held:
+ * gamma_rows is (nrows, nao, nao, nao), row r holding gamma[row0 + r].  Meant
+ * for one atom's segment of the quartet list (every I-shell function of the
+ * quartets inside the rows), so the gradient of a large molecule is streamed
+ * atom block by atom block and never holds the whole [nao]^4 density, as the
+ * reference streams its gradient loop by shell blocks sized from max_memory
+ * (ref: ccsd_gpu/gpu_ccsd_grad.py:416-432).  Functions outside the rows
+ * contribute zero (a bounds guard, not an error).
+ */
+int ccsd_b200_eri_ip1_contract_rows(const int32_t *atm, const int32_t *bas, const double *env,
+                                    const int32_t *ao_loc, int nao, const double *gamma_rows, int row0, int nrows,
+                                    const int32_t *quartets, long long nq, const long long *seg, int nseg, int lmax,
+                                    double *qwork, double *out, void *stream);
+
+/*
  * Failure-path probe (no counterpart in the reference): one thread waits,
  * with the same bounded mbarrier wait the tensor-core GEMM pipeline uses, on
  * a barrier that nothing arrives at.  After limit_ns (<= 10 s) of global
