@@ -14,7 +14,7 @@ from types import SimpleNamespace
 import numpy as np
 import torch
 
-from . import _native
+from . import _native, lowmem
 from .contract import check_status, contract, effective_mode
 from .graphs import StepGraph, graph_cache_ok, solve_step
 
@@ -34,18 +34,55 @@ def ao2mo_gpu(mf, mo_coeff=None, frozen=0):
     dm = 2 * C[:, :nocc_all] @ C[:, :nocc_all].T
     C = C[:, frozen:]
     nocc = nocc_all - frozen
-    g = torch.einsum("pqrs,pi->iqrs", mf.eri, C)
-    g = torch.einsum("iqrs,qj->ijrs", g, C)
-    g = torch.einsum("ijrs,rk->ijks", g, C)
-    g = torch.einsum("ijks,sl->ijkl", g, C)
     fock = C.T @ (mf.get_hcore() + mf.get_veff(dm=dm)) @ C
     o, v = slice(0, nocc), slice(nocc, C.shape[1])
-    e = SimpleNamespace(fock=fock, mo_energy=torch.diagonal(fock).clone(), oooo=g[o, o, o, o].contiguous(),
-                        ovoo=g[o, v, o, o].contiguous(), ovvo=g[o, v, v, o].contiguous(),
-                        oovv=g[o, o, v, v].contiguous(), ovov=g[o, v, o, v].contiguous(),
-                        ovvv=g[o, v, v, v].contiguous(), vvvv=g[v, v, v, v].contiguous())
-    del g
+    if lowmem.lean(4, C.shape[0], C.device):
+        blocks = _mo_blocks_lean(mf.eri, C, nocc)
+        # the CC solves never read the AO ERIs: release them (and the SCF's
+        # cached G) for the solves; mf.eri recomputes them when the gradient
+        # asks (the AO ERIs are the largest tensor of the chain)
+        if hasattr(mf, "_eri"):
+            mf._eri = None
+            mf._G = None
+            torch.cuda.empty_cache()
+    else:
+        g = torch.einsum("pqrs,pi->iqrs", mf.eri, C)
+        g = torch.einsum("iqrs,qj->ijrs", g, C)
+        g = torch.einsum("ijrs,rk->ijks", g, C)
+        g = torch.einsum("ijks,sl->ijkl", g, C)
+        blocks = dict(oooo=g[o, o, o, o].contiguous(), ovoo=g[o, v, o, o].contiguous(),
+                      ovvo=g[o, v, v, o].contiguous(), oovv=g[o, o, v, v].contiguous(),
+                      ovov=g[o, v, o, v].contiguous(), ovvv=g[o, v, v, v].contiguous(),
+                      vvvv=g[v, v, v, v].contiguous())
+        del g
+    e = SimpleNamespace(fock=fock, mo_energy=torch.diagonal(fock).clone(), **blocks)
     return DeviceEris(e)
+
+
+def _mo_blocks_lean(eri, C, nocc):
+    """The seven MO blocks without the (nmo,)*4 tensor: the rows with an
+    occupied first index (nocc x nmo^3) and the vvvv rows, each built block by
+    block from the AO ERIs (lowmem.transform_rows), so only the AO ERIs, the
+    blocks and one row block are live."""
+    nmo = C.shape[1]
+    nvir = nmo - nocc
+    bs = lowmem.block_size(max(C.shape[0], nmo))
+    go = torch.empty((nocc, nmo, nmo, nmo), dtype=C.dtype, device=C.device)
+    for i0 in range(0, nocc, bs):
+        i1 = min(nocc, i0 + bs)
+        go[i0:i1] = lowmem.transform_rows(eri, C[:, i0:i1], C, C, C)
+    o, v = slice(0, nocc), slice(nocc, nmo)
+    out = dict(oooo=go[:, o, o, o].contiguous(), ovoo=go[:, v, o, o].contiguous(), ovvo=go[:, v, v, o].contiguous(),
+               oovv=go[:, o, v, v].contiguous(), ovov=go[:, v, o, v].contiguous(),
+               ovvv=go[:, v, v, v].contiguous())
+    del go
+    Cv = C[:, nocc:]
+    vvvv = torch.empty((nvir,) * 4, dtype=C.dtype, device=C.device)
+    for a0 in range(0, nvir, bs):
+        a1 = min(nvir, a0 + bs)
+        vvvv[a0:a1] = lowmem.transform_rows(eri, Cv[:, a0:a1], Cv, Cv, Cv)
+    out["vvvv"] = vvvv
+    return out
 
 
 def _E(mode):
@@ -190,6 +227,7 @@ class CCSD:
 
     def kernel(self, t1=None, t2=None, eris=None):
         eris = self.ao2mo() if eris is None else DeviceEris.wrap(eris)
+        lowmem.tidy(self.mol.nao_nr())
         nocc = self.nocc
         eo, ev = eris.mo_energy[:nocc], eris.mo_energy[nocc:]
         eia = eo[:, None] - ev[None, :]
@@ -249,6 +287,7 @@ class CCSD:
         return self._scf.e_tot + self.e_corr
 
     def solve_lambda(self, t1=None, t2=None, l1=None, l2=None, eris=None):
+        lowmem.tidy(self.mol.nao_nr())
         return solve_lambda_gpu(self, t1, t2, l1, l2, eris=self.ao2mo() if eris is None else eris,
                                 mode=self.precision)
 

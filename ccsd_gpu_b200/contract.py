@@ -247,11 +247,53 @@ def _combine(terms):
     return x
 
 
+# FP64 contractions whose largest operand exceeds this many bytes are done in
+# slices of that operand along an output index (einsum may copy a permuted
+# operand whole: 21.6 GB for the nvir 228 vvvv block)
+_FP64_SLICE_BYTES = 4 << 30
+
+
+def _fp64_sliced(spec, ta, tb, shape_map, out, alpha, beta):
+    """The FP64 contraction with its largest operand cut into ~1 GB slices
+    along an output index that only that operand carries; None when no slicing
+    is needed or possible.  Each slice's einsum copies at most the slice."""
+    na = max(t.numel() for _, t in ta)
+    nb = max(t.numel() for _, t in tb)
+    if max(na, nb) * 8 <= _FP64_SLICE_BYTES:
+        return None
+    sa, sb, so = _parse(spec)
+    big_a = na >= nb
+    sub_big, terms_big, sub_small = (sa, ta, sb) if big_a else (sb, tb, sa)
+    ix = next((i for i in so if i in sub_big and i not in sub_small), None)
+    if ix is None:
+        return None
+    n = shape_map[ix]
+    chunk = max(1, int((1 << 30) // (8 * max(na, nb) / n)))
+    if out is None:
+        out = torch.empty([shape_map[i] for i in so], dtype=torch.float64, device=ta[0][1].device)
+        beta = 0.0
+    po, pb = so.index(ix), sub_big.index(ix)
+    small = _combine(tb if big_a else ta)
+    for c0 in range(0, n, chunk):
+        m = min(chunk, n - c0)
+        big = _combine([(c, t.narrow(pb, c0, m)) for c, t in terms_big])
+        res = torch.einsum(spec, big, small) if big_a else torch.einsum(spec, small, big)
+        o = out.narrow(po, c0, m)
+        if beta == 0.0:
+            o.copy_(res * alpha if alpha != 1.0 else res)
+        else:
+            o.mul_(beta).add_(res, alpha=alpha)
+    return out
+
+
 def _fp64_contract(spec, ta, tb, shape_map, out, alpha, beta):
     """out = alpha * einsum(spec, a, b) + beta * out with torch.einsum (cuBLAS
     DGEMM); two-term operands are formed first, as the FP64 reference path does."""
     STATS["flops"] += 2 * int(np.prod(list(shape_map.values())))
     STATS["gemms"] += 1
+    r = _fp64_sliced(spec, ta, tb, shape_map, out, alpha, beta)
+    if r is not None:
+        return r
     res = torch.einsum(spec, _combine(ta), _combine(tb))
     if beta == 0.0:
         out.copy_(res * alpha if alpha != 1.0 else res)
@@ -280,6 +322,9 @@ def contract(spec, a, b, out=None, alpha=1.0, beta=0.0, mode="tf32x3", stream=No
         # in-place writes, so it runs under torch.func.vmap (batched solves)
         STATS["flops"] += 2 * int(np.prod(list(shape_map.values())))
         STATS["gemms"] += 1
+        r = _fp64_sliced(spec, ta, tb, shape_map, None, alpha, 0.0)
+        if r is not None:
+            return r
         res = torch.einsum(spec, _combine(ta), _combine(tb))
         return res * alpha if alpha != 1.0 else res
     if out is None:

@@ -25,10 +25,10 @@ this hand-written adjoint (Lambda + RDM + int2e_ip1 . Gamma + Z-vector).
 import numpy as np
 import torch
 
-from . import _native
-from .contract import check_status, contract
+from . import _native, lowmem
+from .contract import check_status, clear_pack_cache, contract
 from .gpu_ccsd_lambda import device_amp
-from .cuda.ip1_contract import contract_int2e_ip1
+from .cuda.ip1_contract import contract_int2e_ip1, contract_int2e_ip1_rows
 from .int1e import intor1e
 
 
@@ -114,7 +114,9 @@ def _gamma2_intermediates_gpu(mycc, t1, t2, l1, l2):
     E("dlia,jlbd->ijab", [(1.0, pvoOV), (0.5, pvOOv)], t2, out=goovv, beta=1.0)
     dovov = 2 * goovv.permute(0, 2, 1, 3) - goovv.permute(1, 2, 0, 3)
     gvvvv = E("ijab,ijcd->abcd", l2, tau)          # l2 . (t2 + t1 t1)
-    dvvvv = gvvvv.permute(0, 2, 1, 3) - 0.5 * gvvvv.permute(0, 3, 1, 2)
+    dvvvv = torch.empty_like(gvvvv)                 # one nvir^4 temporary at most
+    dvvvv.copy_(gvvvv.permute(0, 2, 1, 3))
+    dvvvv.sub_(gvvvv.permute(0, 3, 1, 2), alpha=0.5)
     del gvvvv
     # gvovv[a,i,b,c] = -sum_d gvvvv[a,d,b,c] t1[i,d], evaluated as
     # -sum_kl (sum_d l2[k,l,a,d] t1[i,d]) tau[k,l,b,c]: one tensor-core GEMM
@@ -132,6 +134,14 @@ def _gamma2_intermediates_gpu(mycc, t1, t2, l1, l2):
 
 
 def _rdm2_mo(d2):
+    """Full MO 2-RDM in the reference's layout (ref: ccsd_gpu/gpu_ccsd_grad.py:272-311)."""
+    return _rdm2_mo_raw(d2).permute(1, 0, 3, 2)
+
+
+def _rdm2_mo_raw(d2):
+    """The MO 2-RDM before the final (1, 0, 3, 2) index permutation, contiguous.
+    The symmetrised AO 2-RDM (``_rdm2_ao``) is the same from either, since its
+    symmetrisation over (p <-> q) and (r <-> s) absorbs that permutation."""
     dovov, dvvvv, doooo, doovv, dovvo, _, dovvv, dooov = d2
     nocc, nvir = dovov.shape[:2]
     n = nocc + nvir
@@ -143,7 +153,11 @@ def _rdm2_mo(d2):
     dm2[v, v, o, o] = dm2[o, o, v, v].permute(2, 3, 0, 1)
     dm2[o, v, v, o] = dovvo + dovvo.permute(3, 2, 1, 0)
     dm2[v, o, o, v] = dm2[o, v, v, o].permute(1, 0, 3, 2)
-    dm2[v, v, v, v] = 2 * (dvvvv + dvvvv.permute(1, 0, 3, 2))
+    # the nvir^4 block in place (no nvir^4 temporaries)
+    vvvv = dm2[v, v, v, v]
+    vvvv.copy_(dvvvv)
+    vvvv.add_(dvvvv.permute(1, 0, 3, 2))
+    vvvv.mul_(2.0)
     dm2[o, o, o, o] = 2 * (doooo + doooo.permute(1, 0, 3, 2))
     dm2[o, v, v, v] = dovvv
     dm2[v, v, o, v] = dovvv.permute(2, 3, 0, 1)
@@ -153,7 +167,31 @@ def _rdm2_mo(d2):
     dm2[o, v, o, o] = dooov.permute(2, 3, 0, 1)
     dm2[o, o, v, o] = dooov.permute(1, 0, 3, 2)
     dm2[v, o, o, o] = dooov.permute(3, 2, 1, 0)
-    return dm2.permute(1, 0, 3, 2)
+    return dm2
+
+
+def _rdm2_ao_rows(M, CaT, p0, p1):
+    """Rows [p0, p1) of the symmetrised AO 2-RDM (``_rdm2_ao``) from the raw MO
+    2-RDM M (``_rdm2_mo_raw``) and CaT = C_active^T, without the (nao,)*4
+    tensor: rows and columns of the AO transform (lowmem.transform_rows and
+    transform_cols1), then the (p <-> q, r <-> s) symmetrisation of the rows."""
+    g = lowmem.transform_rows(M, CaT[:, p0:p1], CaT, CaT, CaT)
+    g += lowmem.transform_cols1(M, CaT, CaT[:, p0:p1], CaT, CaT)
+    return 0.5 * (g + g.transpose(2, 3))
+
+
+def _add_hf_terms(gam, P, dm1p, r0=0):
+    """gam (rows [r0, r0 + len(gam)) of an (n,)*4 density) += the HF-like
+    products of P and the relaxed density dm1p, symmetrised in k <-> l
+    (ref: ccsd_gpu/gpu_ccsd_grad.py:416-500, de_k and vhf1): broadcast
+    in-place updates, no (n,)*4 temporaries."""
+    Pr, Dr = P[r0:r0 + gam.shape[0]], dm1p[r0:r0 + gam.shape[0]]
+    gam.addcmul_(Pr[:, :, None, None], dm1p[None, None])                        # P_ij D_kl
+    gam.addcmul_(Dr[:, :, None, None], P[None, None])                           # D_ij P_kl
+    gam.addcmul_(Pr[:, None, None, :], dm1p.T[None, :, :, None], value=-0.25)   # P_il D_kj
+    gam.addcmul_(Pr[:, None, :, None], dm1p.T[None, :, None, :], value=-0.25)   # P_ik D_lj
+    gam.addcmul_(Dr[:, None, None, :], P[None, :, :, None], value=-0.25)        # D_il P_jk
+    gam.addcmul_(Dr[:, None, :, None], P[None, :, None, :], value=-0.25)        # D_ik P_jl
 
 
 def _rdm2_ao(d2, mo_coeff):
@@ -195,16 +233,38 @@ def grad_elec_gpu(mycc, t1, t2, l1, l2, atmlst=None, verbose=None):
     if nf < 0 or int(np.shape(t1)[1]) != nmo - nocc:
         raise ValueError("amplitudes do not match the SCF orbitals (only frozen core orbitals are supported)")
     Co, Cv = C[:, :nocc], C[:, nocc:]
-    eri = mf.eri
+    # large molecules (four more (nao,)*4 tensors would not fit): the AO
+    # 2-RDM is never formed whole; it is built atom block by atom block, once
+    # for Imat and once for the ip1 contraction (the reference streams its
+    # gradient by shell blocks, ref: ccsd_gpu/gpu_ccsd_grad.py:416-432)
+    lean = lowmem.lean(4, nao, dev)
+    if lean:
+        clear_pack_cache()
+        if getattr(mycc, "_eris", None) is not None:
+            mycc._eris = None           # rebuilt by mycc.ao2mo() on demand
+        torch.cuda.empty_cache()
+    eri = mf.eri                        # (recomputed here if the ao2mo released it)
     doo, dov, dvo, dvv = _gamma1_intermediates_gpu(mycc, t1, t2, l1, l2)
     d2 = _gamma2_intermediates_gpu(mycc, t1, t2, l1, l2)
-    dm2 = _rdm2_ao(d2, C[:, nf:])
-    del d2
     P = 2 * Co @ Co.T
     atmlst = range(mol.natm) if atmlst is None else atmlst
     off = mol.offset_nr_by_atom()
     de = torch.zeros((mol.natm, 3), dtype=torch.float64, device=dev)
-    Imat = 0.5 * torch.einsum("ipkl,iqkl->pq", eri, dm2)
+    if lean:
+        M = _rdm2_mo_raw(d2)
+        del d2
+        CaT = C[:, nf:].T.contiguous()
+        Imat = torch.zeros((nao, nao), dtype=torch.float64, device=dev)
+        for a in range(mol.natm):
+            p0, p1 = int(off[a][2]), int(off[a][3])
+            if p1 > p0:
+                rows = _rdm2_ao_rows(M, CaT, p0, p1)
+                Imat += 0.5 * torch.einsum("ipkl,iqkl->pq", eri[p0:p1], rows)
+                del rows
+    else:
+        dm2 = _rdm2_ao(d2, C[:, nf:])
+        del d2
+        Imat = 0.5 * torch.einsum("ipkl,iqkl->pq", eri, dm2)
     S = mf.get_ovlp()
     Imat = -(C.T @ Imat @ S @ C)
     dm1mo = torch.zeros((nmo, nmo), dtype=torch.float64, device=dev)
@@ -243,16 +303,21 @@ def grad_elec_gpu(mycc, t1, t2, l1, l2, atmlst=None, verbose=None):
     # dm2 is already symmetric in k <-> l and so are P (x) dm1p and dm1p (x) P
     # (both densities are symmetric); the exchange products are symmetrised
     # term by term.  Broadcast in-place updates: no (nao,)*4 temporaries.
-    gam = dm2
-    del dm2
-    gam.addcmul_(P[:, :, None, None], dm1p[None, None])                       # P_ij D_kl
-    gam.addcmul_(dm1p[:, :, None, None], P[None, None])                       # D_ij P_kl
-    gam.addcmul_(P[:, None, None, :], dm1p.T[None, :, :, None], value=-0.25)   # P_il D_kj
-    gam.addcmul_(P[:, None, :, None], dm1p.T[None, :, None, :], value=-0.25)   # P_ik D_lj
-    gam.addcmul_(dm1p[:, None, None, :], P[None, :, :, None], value=-0.25)     # D_il P_jk
-    gam.addcmul_(dm1p[:, None, :, None], P[None, :, None, :], value=-0.25)     # D_ik P_jl
-    de -= contract_int2e_ip1(mol, gam)
-    del gam
+    if lean:
+        for a in range(mol.natm):
+            p0, p1 = int(off[a][2]), int(off[a][3])
+            if p1 > p0:
+                rows = _rdm2_ao_rows(M, CaT, p0, p1)
+                _add_hf_terms(rows, P, dm1p, p0)
+                de[a] -= contract_int2e_ip1_rows(mol, rows, a)
+                del rows
+        del M
+    else:
+        gam = dm2
+        del dm2
+        _add_hf_terms(gam, P, dm1p)
+        de -= contract_int2e_ip1(mol, gam)
+        del gam
     charges = mol.atom_charges()
     for a in atmlst:
         _, _, p0, p1_ = (int(v) for v in off[a])

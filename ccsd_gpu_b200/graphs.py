@@ -88,8 +88,16 @@ _SOLVE_GRAPHS_MAX = 32
 GRAPH_MAX_LADDER_FLOPS = 1e12
 
 
+# FP64 bodies are captured only while their vvvv block is below this size: a
+# captured graph keeps its memory pool (the body's temporaries) for as long
+# as the cache holds it, and at large nvir that pool is tens of GB
+GRAPH_MAX_FP64_VVVV_BYTES = 4e9
+
+
 def graph_cache_ok(mode, nocc, nvir):
-    return mode == "fp64" or 2.0 * nocc * nocc * float(nvir) ** 4 < GRAPH_MAX_LADDER_FLOPS
+    if mode == "fp64":
+        return 8.0 * float(nvir) ** 4 < GRAPH_MAX_FP64_VVVV_BYTES
+    return 2.0 * nocc * nocc * float(nvir) ** 4 < GRAPH_MAX_LADDER_FLOPS
 
 
 def solve_step(key, fn, consts, enabled=True):

@@ -2,8 +2,8 @@
 the CPU, examples/h2o_ccsd_grad.py:118-121).
 
 ERIs come from :func:`full_eri_gpu` (each unique shell quartet computed once)
-and stay resident as a dense (nao,)*4 FP64 tensor (that fits HBM for every molecule of the
-configurations: (H2O)6/cc-pVDZ, nao = 144, is 3.4 GB).  J/K, DIIS and the
+and stay resident as a dense (nao,)*4 FP64 tensor ((H2O)6/cc-pVDZ, nao = 144:
+3.4 GB; nao = 288: 55 GB).  J/K, DIIS and the
 eigen-solves are FP64 on the device.  The object exposes the attributes the
 CCSD gradient reads from a PySCF RHF: mol, mo_energy, mo_coeff, mo_occ, e_tot,
 make_rdm1, get_ovlp, get_hcore, get_veff, energy_nuc.
@@ -13,7 +13,7 @@ from types import SimpleNamespace
 import numpy as np
 import torch
 
-from . import _native, tune
+from . import _native, lowmem, tune
 from .cuda.basis import _check_mol, get_basis_cached, upload_geometry
 from .int1e import intor1e
 
@@ -58,10 +58,9 @@ def full_eri_gpu(mol):
     if mol.cart:
         return g
     T = torch.as_tensor(topo.sph()["C"], dtype=torch.float64, device=dev)      # (ncart, nsph)
-    g = torch.einsum("ap,abcd->pbcd", T, g)
-    g = torch.einsum("bq,pbcd->pqcd", T, g)
-    g = torch.einsum("cr,pqcd->pqrd", T, g)
-    return torch.einsum("ds,pqrd->pqrs", T, g).contiguous()
+    # blocked over the first spherical index: only the Cartesian tensor, the
+    # spherical one and one block are live
+    return lowmem.transform_all(g, T)
 
 
 class RHF:
@@ -95,24 +94,34 @@ class RHF:
 
     def get_jk(self, mol=None, dm=None):
         dm = torch.as_tensor(dm, dtype=torch.float64, device=self.eri.device)
-        return (torch.einsum("pqrs,rs->pq", self.eri, dm), torch.einsum("prqs,rs->pq", self.eri, dm))
+        return lowmem.jk_blocked(self.eri, dm)
 
     def _coulomb_exchange(self):
         """G[pq, rs] = (pq|rs) - 1/2 (pr|qs) as an (n^2, n^2) matrix, built once
         per geometry: each Fock build is then one matrix-vector product that
-        streams G at HBM bandwidth instead of a strided exchange contraction."""
-        if getattr(self, "_G", None) is None:
+        streams G at HBM bandwidth instead of a strided exchange contraction.
+        None when a second (n,)*4 tensor would crowd out the later stages (the
+        ao2mo and the gradient need about three more): J/K then come from the
+        ERIs directly (lowmem.jk_blocked)."""
+        if getattr(self, "_G", None) is None and not getattr(self, "_no_G", False):
             e = self.eri
             n = e.shape[0]
+            if lowmem.lean(3, n, e.device):
+                self._no_G = True
+                return None
             g = e.clone()
             g.sub_(e.permute(0, 2, 1, 3), alpha=0.5)
             self._G = g.view(n * n, n * n)
-        return self._G
+        return getattr(self, "_G", None)
 
     def get_veff(self, mol=None, dm=None):
         dm = torch.as_tensor(dm, dtype=torch.float64, device=self.eri.device)
         n = dm.shape[0]
-        return (self._coulomb_exchange() @ dm.reshape(n * n)).view(n, n)
+        G = self._coulomb_exchange()
+        if G is None:
+            J, K = lowmem.jk_blocked(self.eri, dm)
+            return J - 0.5 * K
+        return (G @ dm.reshape(n * n)).view(n, n)
 
     def energy_nuc(self):
         return self.mol.energy_nuc()

@@ -1,6 +1,11 @@
 import os
 import sys
 
+# expandable allocator segments (set before CUDA starts): the bounded-memory
+# test of a nao 288 gradient frees and allocates tensors of tens of GB, which
+# a segment-splitting cache fragments
+os.environ.setdefault("PYTORCH_CUDA_ALLOC_CONF", "expandable_segments:True")
+
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
