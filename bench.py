@@ -279,6 +279,19 @@ def _events_timed(fn, steps, barrier, flush=None):
     return np.array([a.elapsed_time(b) for a, b in evs]), t0.elapsed_time(t1)
 
 
+def release_caches(dev):
+    """Drop the package's device caches (captured solve graphs, packed
+    split-precision operands) between workloads of one run."""
+    import gc
+    from ccsd_gpu_b200 import batch, contract, graphs
+    batch.clear_graphs()
+    graphs.clear_solve_graphs()
+    contract.clear_pack_cache()
+    gc.collect()
+    torch.cuda.synchronize(dev)
+    torch.cuda.empty_cache()
+
+
 def _maxr(x, ws, dev):
     if ws == 1:
         return x
@@ -358,43 +371,96 @@ def _rel(a, b):
     return d / m if m > 0 else d
 
 
-def run_lambda(args, ws, rank, local):
-    """Lambda/2-RDM contraction bench on a synthetic CCSD state."""
+def _lambda_solver(t1, t2, deris, iters, keep):
     from types import SimpleNamespace
-    from ccsd_gpu_b200 import workloads
-    from ccsd_gpu_b200.contract import STATS, check_status, reset_stats
     from ccsd_gpu_b200.gpu_ccsd_grad import _gamma1_intermediates_gpu, _gamma2_intermediates_gpu
-    from ccsd_gpu_b200.gpu_ccsd_lambda import DeviceEris, make_intermediates_gpu, update_lambda_gpu
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    barrier = (lambda: (torch.distributed.barrier(), torch.cuda.synchronize(dev))) if ws > 1 else \
-        (lambda: torch.cuda.synchronize(dev))
-    eris, t1, t2 = workloads.lambda_bench_state(args.nocc, args.nvir, seed=rank, device=dev)
-    deris = DeviceEris(eris, dev)
-    del eris
-    keep = {}
+    from ccsd_gpu_b200.gpu_ccsd_lambda import make_intermediates_gpu, update_lambda_gpu
 
     def solve(mode):
         cc = SimpleNamespace(level_shift=0.0, precision=mode)
         imds = make_intermediates_gpu(cc, t1, t2, deris, mode)
         l1, l2 = t1, t2
-        for _ in range(args.iters):
+        for _ in range(iters):
             l1, l2 = update_lambda_gpu(cc, t1, t2, l1, l2, deris, imds, mode=mode)
         d1 = _gamma1_intermediates_gpu(cc, t1, t2, l1, l2)
         d2 = _gamma2_intermediates_gpu(cc, t1, t2, l1, l2)
         keep[mode] = (l1, l2, d1, d2)
+    return solve
 
+
+def lambda_cpu_baseline(args, dev, full_flops, nocc=16, nvir=144):
+    """The oracle's numpy restatement of the reference's Lambda/RDM path
+    (oracle/cc_oracle.py: make_intermediates, update_lambda, gamma1, gamma2, the
+    equations of ref: ccsd_gpu/gpu_ccsd_lambda.py:68-337 and
+    ccsd_gpu/gpu_ccsd_grad.py:101-246) on the host cores, on a bounded sample:
+    the same synthetic state at (nocc, nvir) = (16, 144), intermediates + two
+    timed Lambda iterations (times iterations) + the RDM intermediates.  Scaled
+    to the benchmark's size by the ratio of counted contraction flops of the
+    package's FP64 run at the two sizes (the full-size numpy run needs tens of
+    GB of host temporaries)."""
+    from types import SimpleNamespace
+    from oracle import cc_oracle
+    from ccsd_gpu_b200 import workloads
+    from ccsd_gpu_b200.contract import STATS, reset_stats
+    from ccsd_gpu_b200.gpu_ccsd_lambda import DeviceEris
+    eris, t1, t2 = workloads.lambda_bench_state(nocc, nvir, seed=0, device=dev)
+    h = lambda x: x.detach().cpu().numpy()      # noqa: E731
+    E = SimpleNamespace(**{k: h(getattr(eris, k)) for k in ("oooo", "ovoo", "ovvo", "oovv", "ovov", "ovvv", "vvvv")})
+    fock, moe, t1h, t2h = h(eris.fock), h(eris.mo_energy), h(t1), h(t2)
+    # counted flops of the same run at the sample size (package, FP64)
+    deris = DeviceEris(eris, dev)
+    keep = {}
+    solve = _lambda_solver(t1, t2, deris, args.iters, keep)
+    reset_stats()
+    solve("fp64")
+    torch.cuda.synchronize(dev)
+    small_flops = STATS["flops"]
+    del deris, keep, eris
+    torch.cuda.empty_cache()
+    t0 = time.perf_counter()
+    imds = cc_oracle.make_intermediates(t1h, t2h, fock, E)
+    t_imd = time.perf_counter() - t0
+    l1, l2 = t1h, t2h
+    n_it = 2
+    t0 = time.perf_counter()
+    for _ in range(n_it):
+        l1, l2 = cc_oracle.update_lambda(t1h, t2h, l1, l2, fock, moe, E, imds)
+    t_it = (time.perf_counter() - t0) / n_it
+    t0 = time.perf_counter()
+    cc_oracle.gamma1(t1h, t2h, l1, l2)
+    cc_oracle.gamma2(t1h, t2h, l1, l2)
+    t_rdm = time.perf_counter() - t0
+    t_small = t_imd + args.iters * t_it + t_rdm
+    scale = full_flops / small_flops
+    return {"value": t_small * scale, "unit": "s/run", "cores": os.cpu_count(), "kind": "port",
+            "sample": "numpy oracle at nocc %d, nvir %d: intermediates %.2f s + %d x %.2f s per Lambda iteration "
+                      "(2 timed) + RDM %.2f s = %.1f s, scaled x%.1f by counted contraction flops to nocc %d, "
+                      "nvir %d" % (nocc, nvir, t_imd, args.iters, t_it, t_rdm, t_small, scale, args.nocc, args.nvir)}
+
+
+def measure_lambda(args, ws, rank, dev, steps, warmup, cpu=False):
+    """Configuration 3: intermediates + iters Lambda updates + RDM intermediates
+    of the synthetic (nocc, nvir) state, FP64 and the split mode (dict)."""
+    from ccsd_gpu_b200 import workloads
+    from ccsd_gpu_b200.contract import STATS, check_status, reset_stats
+    from ccsd_gpu_b200.gpu_ccsd_lambda import DeviceEris
+    barrier = _barrier_fn(ws, dev)
+    eris, t1, t2 = workloads.lambda_bench_state(args.nocc, args.nvir, seed=rank, device=dev)
+    deris = DeviceEris(eris, dev)
+    del eris
+    keep = {}
+    solve = _lambda_solver(t1, t2, deris, args.iters, keep)
     out = {}
     for mode in ("fp64", args.mode):
         keep.pop(mode, None)
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             solve(mode)
         reset_stats()
         with ClockSampler(dev) as clk:
-            ks, region = _events_timed(lambda: solve(mode), args.steps, barrier)
+            ks, region = _events_timed(lambda: solve(mode), steps, barrier)
         check_status(dev)
-        out[mode] = {"s_per_run": _maxr(float(ks.mean()), ws, dev) * 1e-3, "flops": STATS["flops"] / args.steps,
-                     "launches": STATS["launches"] // args.steps, "clocks": clk.summary()}
+        out[mode] = {"s_per_run": _maxr(float(ks.mean()), ws, dev) * 1e-3, "flops": STATS["flops"] / steps,
+                     "launches": STATS["launches"] // steps, "clocks": clk.summary()}
         if mode != "fp64":
             ref, got = keep["fp64"], keep[mode]
             d2e = max(_rel(x, y) for x, y in zip(got[3], ref[3]) if x is not None)
@@ -403,26 +469,42 @@ def run_lambda(args, ws, rank, local):
                              rdm1_rel_err=d1e, rdm2_rel_err=d2e)
             del keep["fp64"]
         torch.cuda.empty_cache()
+    del deris, keep, t1, t2
+    torch.cuda.empty_cache()
     fp, mx = out["fp64"], out[args.mode]
     peak, peak_src = _tensor_peak()
     ach = 3 * mx["flops"] / mx["s_per_run"] / 1e12
+    res = {"workload": "lambda_rdm_o%d_v%d" % (args.nocc, args.nvir), "iterations": args.iters,
+           "steps": steps, "warmup": warmup, "fp64": fp, "mixed": mx,
+           "speedup_vs_fp64": fp["s_per_run"] / mx["s_per_run"],
+           "roofline": {"bound": "tensor", "achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak,
+                        "traffic": None, "peak_source": peak_src,
+                        "flops": "3 TF32 products x counted 2 M N K of every contraction in the run"},
+           "cpu_baseline": None}
+    if cpu and rank == 0:
+        res["cpu_baseline"] = lambda_cpu_baseline(args, dev, fp["flops"])
+    return res
+
+
+def run_lambda(args, ws, rank, local):
+    """Lambda/2-RDM contraction bench on a synthetic CCSD state."""
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    r = measure_lambda(args, ws, rank, dev, args.steps, args.warmup, cpu=True)
+    mx = r["mixed"]
     line = {"metric": "Lambda/2-RDM run time (nocc %d, nvir %d, %d Lambda iterations + RDM intermediates), %s vs FP64"
                       % (args.nocc, args.nvir, args.iters, args.mode),
             "value": mx["s_per_run"], "unit": "s/run", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": mx["s_per_run"] * 1e3, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": args.mode, "data": "synthetic",
-            "config": {"workload": "lambda_rdm_o%d_v%d" % (args.nocc, args.nvir), "iterations": args.iters,
+            "config": {"workload": r["workload"], "iterations": args.iters,
                        "state": "seeded synthetic CCSD state (lambda_bench_state)",
                        "l2": "operands larger than L2 (vvvv block 17.4 GB)",
                        "parallelism": "dp%d" % ws if ws > 1 else "single"},
-            "fp64": fp, "mixed": mx, "speedup_vs_fp64": fp["s_per_run"] / mx["s_per_run"],
-            "roofline": {"bound": "tensor", "achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak,
-                         "traffic": None, "peak_source": peak_src,
-                         "flops": "3 TF32 products x counted 2 M N K of every contraction in the run"},
-            "gpu_launches": mx["launches"], "clocks": mx["clocks"], "cpu_baseline": None, "e2e": None}
+            "fp64": r["fp64"], "mixed": mx, "speedup_vs_fp64": r["speedup_vs_fp64"], "roofline": r["roofline"],
+            "gpu_launches": mx["launches"], "clocks": mx["clocks"], "cpu_baseline": r["cpu_baseline"], "e2e": None}
     if rank == 0:
         print(json.dumps(line), flush=True)
-
 
 
 H2O_CCPVDZ = "O 0 0 0; H 0 0.757 0.587; H 0 -0.757 0.587"
@@ -598,15 +680,13 @@ def _ccsd_energy(mol, mode):
     return cc.e_tot
 
 
-def run_autograd(args, ws, rank, local):
-    """CCSDEnergy forward + backward for ethanol/cc-pVDZ; central-FD check."""
+def measure_autograd(args, ws, rank, dev, steps, warmup, fd=True):
+    """Configuration 4: CCSDEnergy forward + backward for ethanol/cc-pVDZ, FP64
+    and the split mode, and a central-FD check of the backward (dict)."""
     from ccsd_gpu_b200 import workloads
     from ccsd_gpu_b200.gpu_ccsd_grad import CCSDEnergy
     from ccsd_gpu_b200.gto import M
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    barrier = (lambda: (torch.distributed.barrier(), torch.cuda.synchronize(dev))) if ws > 1 else \
-        (lambda: torch.cuda.synchronize(dev))
+    barrier = _barrier_fn(ws, dev)
     sym, xyz = workloads.ethanol_atoms(seed=0)
     mol = M(atom=workloads.atom_string(sym, xyz), basis="cc-pvdz")
     x0 = torch.tensor(mol.atom_coords(), dtype=torch.float64)
@@ -623,15 +703,15 @@ def run_autograd(args, ws, rank, local):
     res = {}
     for mode in ("fp64", args.mode):
         fn = step(mode)
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             fn()
         with ClockSampler(dev) as clk:
-            ks, _ = _events_timed(fn, args.steps, barrier)
+            ks, _ = _events_timed(fn, steps, barrier)
         res[mode] = {"s_per_grad": _maxr(float(ks.mean()), ws, dev) * 1e-3, "clocks": clk.summary()}
     fd_err = None
-    if not args.no_fd and rank == 0:
+    if fd and rank == 0:
         h = 1e-3
-        fd = np.zeros_like(grads["fp64"])
+        fdg = np.zeros_like(grads["fp64"])
         for a in range(mol.natm):
             for c in range(3):
                 ep = []
@@ -639,28 +719,40 @@ def run_autograd(args, ws, rank, local):
                     xs = x0.numpy().copy()
                     xs[a, c] += sgn * h
                     ep.append(_ccsd_energy(mol.copy().set_geom_(xs), "fp64"))
-                fd[a, c] = (ep[0] - ep[1]) / (2 * h)
-        fd_err = {"max_abs_fd_minus_fp64_backward": float(np.abs(fd - grads["fp64"]).max()),
-                  "max_abs_fd_minus_mixed_backward": float(np.abs(fd - grads[args.mode]).max()),
-                  "step_bohr": h, "coordinates": int(fd.size)}
-    mx = res[args.mode]
+                fdg[a, c] = (ep[0] - ep[1]) / (2 * h)
+        fd_err = {"max_abs_fd_minus_fp64_backward": float(np.abs(fdg - grads["fp64"]).max()),
+                  "max_abs_fd_minus_mixed_backward": float(np.abs(fdg - grads[args.mode]).max()),
+                  "step_bohr": h, "coordinates": int(fdg.size)}
+    return {"workload": "ethanol_ccpvdz_autograd", "nao": mol.nao_nr(), "nocc": mol.nelectron // 2,
+            "steps": steps, "warmup": warmup,
+            "fp64_grads_per_s": ws / res["fp64"]["s_per_grad"], "mixed_grads_per_s": ws / res[args.mode]["s_per_grad"],
+            "speedup_vs_fp64": res["fp64"]["s_per_grad"] / res[args.mode]["s_per_grad"],
+            "max_abs_dg_vs_fp64": float(np.abs(grads[args.mode] - grads["fp64"]).max()),
+            "finite_difference": fd_err, "fp64": res["fp64"], "mixed": res[args.mode]}
+
+
+def run_autograd(args, ws, rank, local):
+    """CCSDEnergy forward + backward for ethanol/cc-pVDZ; central-FD check."""
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    r = measure_autograd(args, ws, rank, dev, args.steps, args.warmup, fd=not args.no_fd)
+    mx = r["mixed"]
     line = {"metric": "CCSDEnergy forward+backward per s, ethanol/cc-pVDZ, %s vs FP64" % args.mode,
-            "value": ws / mx["s_per_grad"], "unit": "grads/s", "n_gpus": ws, "steps": args.steps,
+            "value": r["mixed_grads_per_s"], "unit": "grads/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": mx["s_per_grad"] * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": args.mode, "data": "synthetic",
-            "config": {"workload": "ethanol_ccpvdz_autograd", "fp64_polish": args.polish, "nao": mol.nao_nr(), "nocc": mol.nelectron // 2,
+            "config": {"workload": r["workload"], "fp64_polish": args.polish, "nao": r["nao"], "nocc": r["nocc"],
                        "geometry": "standard internal coordinates + N(0, 0.02 A) displacements, seed 0",
                        "parallelism": "dp%d" % ws if ws > 1 else "single"},
-            "fp64_grads_per_s": ws / res["fp64"]["s_per_grad"], "mixed_grads_per_s": ws / mx["s_per_grad"],
-            "speedup_vs_fp64": res["fp64"]["s_per_grad"] / mx["s_per_grad"],
-            "max_abs_dg_vs_fp64": float(np.abs(grads[args.mode] - grads["fp64"]).max()),
-            "finite_difference": fd_err, "roofline": None, "clocks": mx["clocks"], "cpu_baseline": None,
-            "e2e": None}
+            "fp64_grads_per_s": r["fp64_grads_per_s"], "mixed_grads_per_s": r["mixed_grads_per_s"],
+            "speedup_vs_fp64": r["speedup_vs_fp64"], "max_abs_dg_vs_fp64": r["max_abs_dg_vs_fp64"],
+            "finite_difference": r["finite_difference"], "roofline": None, "clocks": mx["clocks"],
+            "cpu_baseline": None, "e2e": None}
     if rank == 0:
         print(json.dumps(line), flush=True)
 
 
-def measure_clusters(args, ws, rank, dev, nmol):
+def measure_clusters(args, ws, rank, dev, nmol, dropin=False):
     """Configuration 5: gradients of the seeded (H2O)n clusters (n in 1..6),
     FP64 mode and the split-precision mode.  Rank r takes clusters r, r + N,
     ... of the first nmol.  One warm-up pass over one cluster of each size
@@ -687,6 +779,20 @@ def measure_clusters(args, ws, rank, dev, nmol):
             b.record()
             barrier()
         res[mode] = {"s_per_pass": _maxr(a.elapsed_time(b) * 1e-3, ws, dev), "clocks": clk.summary()}
+    if dropin:
+        # the plain FP64 drop-in path: one molecule after another through the
+        # FP64 chain (no shape batching), as the reference runs one molecule
+        batch.gradients(warm, "fp64", polish=args.polish, batched=False)
+        with ClockSampler(dev) as clk:
+            barrier()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            gd = batch.gradients(mols, "fp64", polish=args.polish, batched=False)
+            b.record()
+            barrier()
+        res["fp64_dropin"] = {"s_per_pass": _maxr(a.elapsed_time(b) * 1e-3, ws, dev), "clocks": clk.summary(),
+                              "max_abs_dg_vs_batched_fp64": max(float(np.abs(x - y).max())
+                                                                for x, y in zip(gd, grads["fp64"]))}
     dg = [float(np.abs(x - y).max()) for x, y in zip(grads[args.mode], grads["fp64"])]
     total = len(allc[:nmol]) if nmol <= 64 else nmol
     return {"workload": "water_clusters_ccpvdz", "molecules": total, "molecules_per_rank": len(mols),
@@ -696,14 +802,18 @@ def measure_clusters(args, ws, rank, dev, nmol):
             "mixed_molecules_per_s": total / res[args.mode]["s_per_pass"],
             "speedup_vs_fp64": res["fp64"]["s_per_pass"] / res[args.mode]["s_per_pass"],
             "per_molecule_max_abs_dg_vs_fp64": dg, "max_abs_dg_vs_fp64": max(dg),
-            "fp64": res["fp64"], "mixed": res[args.mode]}
+            "fp64": res["fp64"], "mixed": res[args.mode],
+            "fp64_dropin": res.get("fp64_dropin"),
+            "fp64_dropin_molecules_per_s": total / res["fp64_dropin"]["s_per_pass"] if dropin else None,
+            "speedup_vs_fp64_dropin": (res["fp64_dropin"]["s_per_pass"] / res[args.mode]["s_per_pass"]
+                                       if dropin else None)}
 
 
 def run_clusters(args, ws, rank, local):
     """Gradients of seeded water clusters, FP64 and split precision."""
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    r = measure_clusters(args, ws, rank, dev, args.molecules)
+    r = measure_clusters(args, ws, rank, dev, args.molecules, dropin=True)
     mx = r["mixed"]
     line = {"metric": "CCSD gradients of (H2O)n clusters, n in 1..6, cc-pVDZ: molecules/s, %s vs FP64" % args.mode,
             "value": r["mixed_molecules_per_s"], "unit": "molecules/s", "n_gpus": ws,
@@ -716,6 +826,8 @@ def run_clusters(args, ws, rank, local):
                        "parallelism": "dp%d" % ws if ws > 1 else "single"},
             "fp64_molecules_per_s": r["fp64_molecules_per_s"], "mixed_molecules_per_s": r["mixed_molecules_per_s"],
             "speedup_vs_fp64": r["speedup_vs_fp64"],
+            "fp64_dropin_molecules_per_s": r["fp64_dropin_molecules_per_s"],
+            "speedup_vs_fp64_dropin": r["speedup_vs_fp64_dropin"],
             "per_molecule_max_abs_dg_vs_fp64": r["per_molecule_max_abs_dg_vs_fp64"],
             "max_abs_dg_vs_fp64": r["max_abs_dg_vs_fp64"],
             "roofline": None, "clocks": mx["clocks"], "cpu_baseline": None, "e2e": None}
@@ -867,15 +979,21 @@ def main():
         "parity_vs_reference": parity,
     }
     if not args.no_molecules:
-        # the metric's gradient clauses, measured after (outside) the ERI timed
-        # region: configuration 1 (H2O/cc-pVDZ) and configuration 5 (the 64
-        # seeded water clusters), FP64 mode against the split-precision mode
+        # the metric's other clauses, measured after (outside) the ERI timed
+        # region: configuration 1 (H2O/cc-pVDZ gradient), configuration 5 (the
+        # 64 seeded water clusters), configuration 4 (ethanol CCSDEnergy forward
+        # + backward, FD-checked) and, from released caches, configuration 3
+        # (Lambda/RDM contractions, nocc 24, nvir 216); FP64 mode against the
+        # split-precision mode
         h2o = measure_h2o(args, ws, rank, dev, steps=10, warmup=3)
         for k in ("mixed", "fp64"):
             h2o[k].pop("clocks", None)
         line["h2o_ccpvdz_gradient"] = h2o
-        cl = measure_clusters(args, ws, rank, dev, 64)
+        cl = measure_clusters(args, ws, rank, dev, 64, dropin=True)
         line["water_clusters_gradient"] = cl
+        line["ethanol_ccpvdz_autograd"] = measure_autograd(args, ws, rank, dev, steps=2, warmup=1, fd=True)
+        release_caches(dev)
+        line["lambda_rdm"] = measure_lambda(args, ws, rank, dev, steps=1, warmup=1, cpu=False)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if ws > 1:
