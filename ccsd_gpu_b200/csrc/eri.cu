@@ -215,8 +215,9 @@ static int launch_main_dl(Kind k, const EriArgs &a, long long grid, size_t smem,
 static int run_pair(Kind k, int deriv, bool low, const EriArgs &a, long long nwork, long long nheavy,
                     cudaStream_t st)
 {
-    const size_t smem = (size_t)a.smem_warp * kWarps * sizeof(double);
-    long long grid = (nwork + kWarps - 1) / kWarps;
+    const int nw = warps_of(k == Kind::GRAD ? MODE_GRAD : (k == Kind::FULL ? MODE_FULL : MODE_QSUM));
+    const size_t smem = (size_t)a.smem_warp * nw * sizeof(double);
+    long long grid = (nwork + nw - 1) / nw;
     const long long gmax = (long long)num_sms() * 16;
     if (grid > gmax) grid = gmax;
     const size_t hsmem = (size_t)a.smem_heavy * sizeof(double);

@@ -1317,7 +1317,7 @@ __global__ void __launch_bounds__(kWarps * 32, 2) eri_s2kl_kernel(
 // heavy: quartets with more Cartesian functions than this go to the CTA kernel
 // (0: heavy_nf(D)); the CTA kernel of the same list gets the same value.
 template <int D, bool LOW, int MODE = MODE_QSUM>
-__global__ void __launch_bounds__(kWarps * 32, 2) eri_qsum_kernel(
+__global__ void __launch_bounds__(warps_of(MODE) * 32, 8 / warps_of(MODE)) eri_qsum_kernel(
     const int *__restrict__ atm, const int *__restrict__ bas, const double *__restrict__ env,
     const int4 *__restrict__ quartets, long long nq, double *__restrict__ qsum, int smem_warp,
     const int *__restrict__ ao_loc = nullptr, const double *__restrict__ gamma = nullptr, int nao = 0,
@@ -1341,7 +1341,7 @@ __global__ void __launch_bounds__(kWarps * 32, 2) eri_qsum_kernel(
     // code path) at the same time.
     const long long per = (nq + gridDim.x - 1) / gridDim.x;
     const long long t0 = (long long)blockIdx.x * per, t1 = t0 + per < nq ? t0 + per : nq;
-    for (long long t = t0 + warp; t < t1; t += kWarps) {
+    for (long long t = t0 + warp; t < t1; t += warps_of(MODE)) {
         const long long q = nq - 1 - t;
         const int4 s = quartets[q];
         if (quartet_nf(bas, s.x, s.y, s.z, s.w) > heavy) continue;
@@ -1462,7 +1462,7 @@ int launch_list(const EriArgs &a, long long grid, size_t smem, cudaStream_t st)
 {
     int rc;
     if ((rc = prepare_kernel(eri_qsum_kernel<D, LOW, MODE>, smem))) return rc;
-    eri_qsum_kernel<D, LOW, MODE><<<(int)grid, kWarps * 32, smem, st>>>(a.atm, a.bas, a.env, a.quartets, a.nq,
+    eri_qsum_kernel<D, LOW, MODE><<<(int)grid, warps_of(MODE) * 32, smem, st>>>(a.atm, a.bas, a.env, a.quartets, a.nq,
                                                                         a.qsum, a.smem_warp, a.ao_loc, a.gamma,
                                                                         a.nao, a.full, a.heavy, a.grow0, a.grows);
     return check_launch("eri_qsum_kernel");

@@ -6,7 +6,7 @@
 
 namespace cb {
 
-static constexpr int kWarps = 4;          // warps (quartets in flight) per CTA of the warp kernels
+static constexpr int kWarps = 4;          // warps (quartets in flight) per CTA of the warp kernels (default)
 static constexpr int kHeavyThreads = 256; // threads of the CTA (heavy-quartet) kernels
 static constexpr int kMaxSlots = 64;      // slots per batch cap
 static constexpr int kParStride = 13;     // doubles of per-slot parameters (odd: lanes spread over banks)
@@ -21,6 +21,15 @@ static constexpr int kHeavyNfIp1 = 500;
 __host__ __device__ constexpr int heavy_nf(int D) { return D ? kHeavyNfIp1 : kHeavyNf; }
 
 enum { MODE_S2KL = 0, MODE_QSUM = 1, MODE_GRAD = 2, MODE_FULL = 3 };
+
+// Warps per CTA of the warp kernel of an epilogue mode.  The molecular lists
+// (the gradient's ip1-Gamma contraction, the SCF's dense ERI tensor) run
+// 8-warp CTAs, one per SM: every warp of an SM then walks the same part of the
+// class-sorted list and shares one instruction working set (the kernels stall
+// mostly on instruction fetch; measured 11-13% faster on (H2O)n/cc-pVDZ
+// gradient lists, 7-11% on int2e).  The synthetic checksum list and the s2kl
+// blocks keep 4-warp CTAs, two per SM (the checksum list ran 19% slower with 8).
+__host__ __device__ constexpr int warps_of(int mode) { return mode == MODE_GRAD || mode == MODE_FULL ? 8 : kWarps; }
 
 struct EriArgs {
     const int *atm = nullptr, *bas = nullptr;
