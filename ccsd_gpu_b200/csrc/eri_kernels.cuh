@@ -772,8 +772,24 @@ __device__ __forceinline__ void hc_hrr_any(int l0, int l1, const double *__restr
 struct HcPlan {
     int nset, a0[2], ne[2], nf_ket, nacc, setoff[2];
     int nc, nd, ncd, na[2], nb, rowoff[2], nrows, braoff[2], nbra, nket;
+    // grouped accumulation: groups (set, ex, ey, ket component f), members
+    // ez = ez_lo .. ez_lo + ze - 1 (ze = lj + 1); gset0 groups in set 0
+    int ngrp, gset0, ze;
     bool kswap, bswap;
 };
+
+// Which l <= 2 quartets take the contracted-HRR path on a warp (CB_HC_RULE):
+// 0 the measured rule of hc_plan(), 1 every int2e_ip1 quartet that fits,
+// 2 every quartet that fits.
+#ifndef CB_HC_RULE
+#define CB_HC_RULE 0
+#endif
+// Grouped accumulation on the contracted-HRR path (0: one accumulator per
+// [e|f] value and lane, the form before grouping).
+#ifndef CB_HC_GROUPED
+#define CB_HC_GROUPED 1
+#endif
+static constexpr int kHcMaxG = 8;       // groups per lane on a warp (grouped form)
 
 __device__ __forceinline__ bool hc_plan(int D, int li, int lj, int lk, int ll, HcPlan &h,
                                         int maxacc = 32 * kHcMaxJ, int cap = kHcSmem, bool always = false)
@@ -805,10 +821,20 @@ __device__ __forceinline__ bool hc_plan(int D, int li, int lj, int lk, int ll, H
         h.nbra += h.na[s] * h.nb;
     }
     h.nket = h.nrows * h.ncd;
+    h.ze = lj + 1;
+    h.gset0 = 0;
+    h.ngrp = 0;
+    for (int s = 0; s < h.nset; s++) {
+        const int m = h.a0[s] + lj;           // largest |e| of the set
+        const int g = (m + 1) * (m + 2) / 2 * h.nf_ket;
+        if (s == 0) h.gset0 = g;
+        h.ngrp += g;
+    }
     const int nf = hc_ncart(li) * h.nb * h.ncd;
     const int lo = h.nacc > h.nbra * h.ncd ? h.nacc : h.nbra * h.ncd;
     if (h.nacc > maxacc || lo + h.nket > cap) return false;
     if (always) return true;
+    if (CB_HC_RULE == 2 || (CB_HC_RULE == 1 && D)) return true;
     // measured: worth it when the per-output path would recompute the slots
     // for several 256-output chunks, or when [e|f] is clearly smaller than
     // the output block and the ket has no s shell
@@ -822,16 +848,53 @@ __device__ __forceinline__ void grp_sync()
     else __syncthreads();
 }
 
+// Sum of ncart(l) for l = 0..n (tetrahedral numbers; 0 for n = -1).
+__host__ __device__ constexpr int hc_tet(int n) { return (n + 1) * (n + 2) * (n + 3) / 6; }
+
+// Group t of the grouped accumulation: set s, bra exponents ex, ey, members
+// ez = ezlo .. ezlo + nm - 1 (every |e| = ex + ey + ez in [a0[s], a0[s] + lj]),
+// ket component jf of shell F and its flat ket index ff (shells lk.. in order).
+__device__ __forceinline__ void hc_group(const HcPlan &h, int lj, int lk, int t, int &s, int &ex, int &ey,
+                                         int &ezlo, int &nm, int &F, int &jf, int &ff)
+{
+    s = (h.nset > 1 && t >= h.gset0) ? 1 : 0;
+    const int r = t - (s ? h.gset0 : 0);
+    int pe = r / h.nf_ket;
+    ff = r - pe * h.nf_ket;
+    const int m = h.a0[s] + lj;
+    ex = 0;
+    while (pe > m - ex) {
+        pe -= m - ex + 1;
+        ex++;
+    }
+    ey = pe;
+    ezlo = h.a0[s] - ex - ey > 0 ? h.a0[s] - ex - ey : 0;
+    nm = m - ex - ey - ezlo + 1;
+    jf = ff;
+    F = lk;
+    while (jf >= hc_ncart(F)) {
+        jf -= hc_ncart(F);
+        F++;
+    }
+}
+
 // NT cooperating threads (a warp, or a 256-thread CTA for heavy quartets),
 // `cap` doubles of shared memory at wsm; `qsum` is added to (warp) or
 // assigned (CTA) in the checksum and gradient modes.
-template <int D, int MODE, int NJ, int NT>
+//
+// ZE = 0: each lane owns NJ [e|f] accumulators (3 shared-memory loads per
+// value and slot).  ZE > 0 (grouped): each lane owns NJ groups; a group is one
+// (set, ex, ey, ket component f) and its members run over ez (at most ZE = lj
+// + 1 of them), so they share the product Ix(ex, fx) Iy(ey, fy) and read
+// consecutive Iz entries: 2 + (members) loads per group and slot.
+template <int D, int MODE, int NJ, int NT, int ZE = 0>
 __device__ void eri_quartet_hc(const int *__restrict__ atm, const int *__restrict__ bas,
                                const double *__restrict__ env, const int *__restrict__ ao_loc, int ish, int jsh,
                                int ksh, int lsh, const HcPlan &h, double *__restrict__ wsm, const S2klOut &so,
                                double *__restrict__ qsum, int lane, int cap)
 {
     constexpr int NC = D ? 3 : 1;
+    constexpr int NM = ZE ? ZE : 1;
     const Shell si = load_shell(atm, bas, env, h.bswap ? jsh : ish), sj_ = load_shell(atm, bas, env, h.bswap ? ish : jsh);
     const Shell sk_ = load_shell(atm, bas, env, h.kswap ? lsh : ksh), sl_ = load_shell(atm, bas, env, h.kswap ? ksh : lsh);
     const int li = si.l, lj = sj_.l, lk = sk_.l, ll = sl_.l;      // computed orientation
@@ -859,27 +922,40 @@ __device__ void eri_quartet_hc(const int *__restrict__ atm, const int *__restric
     double *gbuf = par + ns * kParStride;
     if (tab) build_pair_tables(si, sj_, sk_, sl_, mb, mk, AB, rab2, CD, rcd2, tab, lane, NT);
 
-    // lane-owned accumulators: flat t = lane + 32 j = setoff[s] + ie * nf_ket + if
+    // ZE = 0: lane-owned accumulators, flat t = lane + NT j = setoff[s] + ie * nf_ket + if,
+    //         idx[j] = x | y << 8 | z << 16 (table offsets) | raised set << 24;
+    // ZE > 0: lane-owned groups t = lane + NT j,
+    //         idx[j] = x | y << 8 | z(ezlo) << 16 | (members - 1) << 24 | raised set << 26
+    const int se = le + 1;
     int idx[NJ];
-    double acc[NJ];
-    const int nj = (h.nacc - lane + NT - 1) / NT;
+    double acc[NJ][NM];
+    const int nj = ((ZE ? h.ngrp : h.nacc) - lane + NT - 1) / NT;
 #pragma unroll
     for (int j = 0; j < NJ; j++) {
-        acc[j] = 0.0;
+#pragma unroll
+        for (int m = 0; m < NM; m++) acc[j][m] = 0.0;
         idx[j] = 0;
         const int t = lane + NT * j;
-        if (t < h.nacc) {
-            const int s = (h.nset > 1 && t >= h.setoff[1]) ? 1 : 0;
-            const int r = t - h.setoff[s];
-            int ie = r / h.nf_ket, jf = r - ie * h.nf_ket;
-            int E = h.a0[s];
-            while (ie >= hc_ncart(E)) { ie -= hc_ncart(E); E++; }
-            int F = lk;
-            while (jf >= hc_ncart(F)) { jf -= hc_ncart(F); F++; }
-            const int ex = hc_lx(E, ie), ey = hc_ly(E, ie), ez = hc_lz(ie);
-            const int fx = hc_lx(F, jf), fy = hc_ly(F, jf), fz = hc_lz(jf);
-            idx[j] = (ex + fx * (le + 1)) | ((ey + fy * (le + 1)) << 8) | ((ez + fz * (le + 1)) << 16) |
-                     ((D && s == 0) ? (1 << 24) : 0);
+        if (j < nj) {
+            if (ZE) {
+                int s, ex, ey, ezlo, nm, F, jf, ff;
+                hc_group(h, lj, lk, t, s, ex, ey, ezlo, nm, F, jf, ff);
+                const int fx = hc_lx(F, jf), fy = hc_ly(F, jf), fz = hc_lz(jf);
+                idx[j] = (ex + fx * se) | ((ey + fy * se) << 8) | ((ezlo + fz * se) << 16) | ((nm - 1) << 24) |
+                         ((D && s == 0) ? (1 << 26) : 0);
+            } else {
+                const int s = (h.nset > 1 && t >= h.setoff[1]) ? 1 : 0;
+                const int r = t - h.setoff[s];
+                int ie = r / h.nf_ket, jf = r - ie * h.nf_ket;
+                int E = h.a0[s];
+                while (ie >= hc_ncart(E)) { ie -= hc_ncart(E); E++; }
+                int F = lk;
+                while (jf >= hc_ncart(F)) { jf -= hc_ncart(F); F++; }
+                const int ex = hc_lx(E, ie), ey = hc_ly(E, ie), ez = hc_lz(ie);
+                const int fx = hc_lx(F, jf), fy = hc_ly(F, jf), fz = hc_lz(jf);
+                idx[j] = (ex + fx * se) | ((ey + fy * se) << 8) | ((ez + fz * se) << 16) |
+                         ((D && s == 0) ? (1 << 24) : 0);
+            }
         }
     }
     for (int s0 = 0; s0 < nslot; s0 += ns) {
@@ -902,8 +978,18 @@ __device__ void eri_quartet_hc(const int *__restrict__ atm, const int *__restric
             for (int j = 0; j < NJ; j++) {
                 if (j < nj) {
                     const int o = idx[j];
-                    const double v = gx[o & 255] * gy[(o >> 8) & 255];
-                    acc[j] = fma(v * gz[(o >> 16) & 255], (o >> 24) ? a2 : 1.0, acc[j]);
+                    if (ZE) {
+                        double v = gx[o & 255] * gy[(o >> 8) & 255];
+                        if (D) v *= ((o >> 26) & 1) ? a2 : 1.0;
+                        const double *zp = gz + ((o >> 16) & 255);
+                        const int nm1 = (o >> 24) & 3;
+#pragma unroll
+                        for (int m = 0; m < NM; m++)
+                            if (m <= nm1) acc[j][m] = fma(v, zp[m], acc[j][m]);
+                    } else {
+                        const double v = gx[o & 255] * gy[(o >> 8) & 255];
+                        acc[j][0] = fma(v * gz[(o >> 16) & 255], (o >> 24) ? a2 : 1.0, acc[j][0]);
+                    }
                 }
             }
         }
@@ -912,8 +998,25 @@ __device__ void eri_quartet_hc(const int *__restrict__ atm, const int *__restric
     // top [cap - nket, cap), bra results at [0, nbra * ncd).
     grp_sync<NT>();
 #pragma unroll
-    for (int j = 0; j < NJ; j++)
-        if (j < nj) wsm[lane + NT * j] = acc[j];
+    for (int j = 0; j < NJ; j++) {
+        if (j < nj) {
+            if (ZE) {
+                int s, ex, ey, ezlo, nm, F, jf, ff;
+                hc_group(h, lj, lk, lane + NT * j, s, ex, ey, ezlo, nm, F, jf, ff);
+                const int base = h.setoff[s] + ff, t0 = hc_tet(h.a0[s] - 1);
+#pragma unroll
+                for (int m = 0; m < NM; m++) {
+                    if (m < nm) {
+                        const int ez = ezlo + m;
+                        const int ie = hc_tet(ex + ey + ez - 1) - t0 + hc_idx(ex, ey, ez);
+                        wsm[base + ie * h.nf_ket] = acc[j][m];
+                    }
+                }
+            } else {
+                wsm[lane + NT * j] = acc[j][0];
+            }
+        }
+    }
     grp_sync<NT>();
     double *ket = wsm + (cap - h.nket);
     for (int row = lane; row < h.nrows; row += NT) {
@@ -1036,6 +1139,25 @@ __device__ void eri_quartet_hc(const int *__restrict__ atm, const int *__restric
     }
 }
 
+// Grouped form: dispatch on the groups per thread (1, 2, 4 or kHcMaxG).
+template <int D, int MODE, int NT, int ZE>
+__device__ __forceinline__ void eri_quartet_hcg(const int *__restrict__ atm, const int *__restrict__ bas,
+                                                const double *__restrict__ env, const int *__restrict__ ao_loc,
+                                                int ish, int jsh, int ksh, int lsh, const HcPlan &h,
+                                                double *__restrict__ wsm, const S2klOut &so,
+                                                double *__restrict__ qsum, int lane, int cap, int ng)
+{
+    if (ng <= 1)
+        eri_quartet_hc<D, MODE, 1, NT, ZE>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, h, wsm, so, qsum, lane, cap);
+    else if (ng <= 2)
+        eri_quartet_hc<D, MODE, 2, NT, ZE>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, h, wsm, so, qsum, lane, cap);
+    else if (ng <= 4 || NT > 32)
+        eri_quartet_hc<D, MODE, 4, NT, ZE>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, h, wsm, so, qsum, lane, cap);
+    else
+        eri_quartet_hc<D, MODE, kHcMaxG, NT, ZE>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, h, wsm, so, qsum, lane,
+                                                 cap);
+}
+
 // Dispatch on the accumulator capacity per thread, so the unrolled per-slot
 // loop carries no predicated-off iterations beyond the next multiple of 8.
 template <int D, int MODE>
@@ -1045,6 +1167,21 @@ __device__ __forceinline__ void eri_quartet_hc_any(const int *__restrict__ atm, 
                                                    double *__restrict__ wsm, const S2klOut &so,
                                                    double *__restrict__ qsum, int lane)
 {
+    if (CB_HC_GROUPED) {
+        const int ng = (h.ngrp + 31) / 32;
+        if (ng <= kHcMaxG) {
+            if (h.ze == 1)
+                eri_quartet_hcg<D, MODE, 32, 1>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, h, wsm, so, qsum, lane,
+                                                kHcSmem, ng);
+            else if (h.ze == 2)
+                eri_quartet_hcg<D, MODE, 32, 2>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, h, wsm, so, qsum, lane,
+                                                kHcSmem, ng);
+            else
+                eri_quartet_hcg<D, MODE, 32, 3>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, h, wsm, so, qsum, lane,
+                                                kHcSmem, ng);
+            return;
+        }
+    }
     const int nj = (h.nacc + 31) / 32;
     if (nj <= 8)
         eri_quartet_hc<D, MODE, 8, 32>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, h, wsm, so, qsum, lane, kHcSmem);
@@ -1069,6 +1206,21 @@ __device__ __forceinline__ void eri_quartet_hc_cta(const int *__restrict__ atm, 
                                                    double *__restrict__ sm, int cap, const S2klOut &so,
                                                    double *__restrict__ qsum)
 {
+    if (CB_HC_GROUPED) {
+        const int ng = (h.ngrp + 255) / 256;
+        if (ng <= 4) {
+            if (h.ze == 1)
+                eri_quartet_hcg<D, MODE, 256, 1>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, h, sm, so, qsum,
+                                                 threadIdx.x, cap, ng);
+            else if (h.ze == 2)
+                eri_quartet_hcg<D, MODE, 256, 2>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, h, sm, so, qsum,
+                                                 threadIdx.x, cap, ng);
+            else
+                eri_quartet_hcg<D, MODE, 256, 3>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, h, sm, so, qsum,
+                                                 threadIdx.x, cap, ng);
+            return;
+        }
+    }
     if (h.nacc <= 256 * 8)
         eri_quartet_hc<D, MODE, 8, 256>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, h, sm, so, qsum, threadIdx.x, cap);
     else
