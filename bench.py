@@ -897,6 +897,7 @@ def main():
     tune.enable(not args.no_tune)
     dshare = float((shells._bas[:, 1][q].max(1) >= 2).mean())
     heavy = {d: tune.tune_eri_heavy(ds, shells._bas, q_dev, d, dshare) for d in (1, 0)}
+    paths = {d: tune.tune_eri_paths(ds, shells._bas, q_dev, d, dshare) for d in (1, 0)}
     ip1 = lambda: quartet_checksums(ds, q_dev, 1, out=out)   # noqa: E731
     for _ in range(args.warmup):
         ip1()
@@ -957,6 +958,9 @@ def main():
         "config": {"workload": "eri_microbench_4096_shells_spd_ip1", "nshell": NSHELL, "quartets_per_rank": nq,
                    "lclasses": int(len(classes)), "schwarz": 1e-12,
                    "heavy_nf": {"int2e": heavy[0], "ip1": heavy[1], "autotuned": not args.no_tune},
+                   "paths": {("int2e", "ip1")[d]: {"contracted_hrr": paths[d].count(1),
+                                                   "per_output": paths[d].count(2),
+                                                   "compiled_rule": paths[d].count(0)} for d in (0, 1)},
                    "l2": "256 MiB buffer written between steps, outside the per-step kernel events",
                    "parallelism": "dp%d" % ws if ws > 1 else "single"},
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",

@@ -22,9 +22,13 @@ SIGNATURES = {
     "ccsd_b200_last_error": (ctypes.c_char_p, []),
     "ccsd_b200_eri_s2kl_cart": (_c_int, [_c_int, _vp, _vp, _vp, _c_int, _vp, _c_int, _c_int, _c_int,
                                          _c_int, _vp, _c_ll, _vp, _vp]),
+    "ccsd_b200_eri_s2kl_sph": (_c_int, [_c_int, _vp, _vp, _vp, _c_int, _vp, _vp, _vp, _c_int, _c_int, _c_int,
+                                        _c_int, _vp, _c_ll, _vp, _vp]),
     "ccsd_b200_eri_quartet_checksums": (_c_int, [_c_int, _vp, _vp, _vp, _vp, _c_ll, _c_int, _vp, _vp]),
     "ccsd_b200_eri_set_heavy_nf": (_c_int, [_c_int, _c_int]),
     "ccsd_b200_eri_get_heavy_nf": (_c_int, [_c_int]),
+    "ccsd_b200_eri_set_paths": (_c_int, [_c_int, _vp, _c_int]),
+    "ccsd_b200_eri_get_paths": (_c_int, [_c_int, _vp, _c_int]),
     "ccsd_b200_cart2sph_s2kl": (_c_int, [_vp, _vp, _vp, _c_int, _c_int, _c_int, _c_int, _c_int,
                                          _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "ccsd_b200_fp64_fma_probe": (_c_int, [_vp, _c_int, _c_int, _vp]),

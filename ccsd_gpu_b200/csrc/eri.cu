@@ -209,12 +209,18 @@ static int launch_main_dl(Kind k, const EriArgs &a, long long grid, size_t smem,
     return CCSD_B200_ERR_ARG;
 }
 
+// Accumulation path per L-class of the warp kernels, per derivative order
+// (all zero: the measured rule); set by the autotuner.
+static PathTable g_paths[2];
+
 // The warp kernel over `nwork` quartets on the caller's stream and, when
 // `nheavy` > 0, the CTA (heavy-quartet) kernel on the auxiliary stream,
 // fork/joined by events so the two overlap.
-static int run_pair(Kind k, int deriv, bool low, const EriArgs &a, long long nwork, long long nheavy,
+static int run_pair(Kind k, int deriv, bool low, const EriArgs &a_in, long long nwork, long long nheavy,
                     cudaStream_t st)
 {
+    EriArgs a = a_in;
+    a.paths = g_paths[deriv ? 1 : 0];
     const int nw = warps_of(k == Kind::GRAD ? MODE_GRAD : (k == Kind::FULL ? MODE_FULL : MODE_QSUM));
     const size_t smem = (size_t)a.smem_warp * nw * sizeof(double);
     long long grid = (nwork + nw - 1) / nw;
@@ -283,6 +289,42 @@ int ccsd_b200_eri_s2kl_cart(int deriv, const int32_t *atm, const int32_t *bas, c
     return run_pair(Kind::S2KL, deriv, lmax <= 2, a, nq, n_heavy, (cudaStream_t)stream);
 }
 
+int ccsd_b200_eri_s2kl_sph(int deriv, const int32_t *atm, const int32_t *bas, const double *env, int nbas,
+                           const int32_t *ao_loc, const int32_t *ao_loc_sph, const double *c2s_d, int ish0, int ish1,
+                           int nao_sph, int lmax, const int32_t *heavy_quartets, long long n_heavy, double *out,
+                           void *stream)
+{
+    if (deriv < 0 || deriv > 1 || !atm || !bas || !env || !ao_loc || !ao_loc_sph || !c2s_d || !out || nbas <= 0 ||
+        ish0 < 0 || ish1 > nbas || ish0 >= ish1 || nao_sph <= 0 || lmax < 0 || n_heavy < 0 ||
+        (n_heavy > 0 && !heavy_quartets)) {
+        set_error("ccsd_b200_eri_s2kl_sph: invalid argument");
+        return CCSD_B200_ERR_ARG;
+    }
+    if (lmax > 2) {
+        set_error("ccsd_b200_eri_s2kl_sph: l = %d > 2 (use ccsd_b200_eri_s2kl_cart + ccsd_b200_cart2sph_s2kl)",
+                  lmax);
+        return CCSD_B200_ERR_UNSUPPORTED;
+    }
+    EriArgs a;
+    a.atm = atm;
+    a.bas = bas;
+    a.env = env;
+    a.ao_loc = ao_loc;
+    a.ish0 = ish0;
+    a.ish1 = ish1;
+    a.nbas = nbas;
+    a.nao = nao_sph;
+    a.out = out;
+    a.quartets = reinterpret_cast<const int4 *>(heavy_quartets);
+    a.nq = n_heavy;
+    a.ao_sph = ao_loc_sph;
+    a.c2s = c2s_d;
+    a.smem_warp = smem_per_warp(lmax, deriv);
+    a.smem_heavy = heavy_smem_doubles(lmax, deriv);
+    const long long nq = (long long)(ish1 - ish0) * nbas * ((long long)nbas * (nbas + 1) / 2);
+    return run_pair(Kind::S2KL, deriv, true, a, nq, n_heavy, (cudaStream_t)stream);
+}
+
 // Heavy-quartet thresholds of the list entry points (quartet checksums, the
 // ip1 gradient contraction, the dense int2e tensor), per derivative order;
 // set by the autotuner.  The s2kl block entry keeps the compiled values (its
@@ -302,6 +344,36 @@ int ccsd_b200_eri_set_heavy_nf(int deriv, int nf)
 int ccsd_b200_eri_get_heavy_nf(int deriv)
 {
     return deriv == 0 || deriv == 1 ? g_heavy_list[deriv] : -1;
+}
+
+int ccsd_b200_eri_set_paths(int deriv, const uint8_t *choice, int n)
+{
+    if (deriv < 0 || deriv > 1 || !choice || n != 81) {
+        set_error("ccsd_b200_eri_set_paths: invalid argument");
+        return CCSD_B200_ERR_ARG;
+    }
+    PathTable t;
+    for (int c = 0; c < 81; c++) {
+        if (choice[c] > 2) {
+            set_error("ccsd_b200_eri_set_paths: choice[%d] = %d (0, 1 or 2)", c, (int)choice[c]);
+            return CCSD_B200_ERR_ARG;
+        }
+        if (choice[c] == 1) t.hc[c >> 6] |= 1ull << (c & 63);
+        if (choice[c] == 2) t.po[c >> 6] |= 1ull << (c & 63);
+    }
+    g_paths[deriv] = t;
+    return CCSD_B200_OK;
+}
+
+int ccsd_b200_eri_get_paths(int deriv, uint8_t *choice, int n)
+{
+    if (deriv < 0 || deriv > 1 || !choice || n != 81) {
+        set_error("ccsd_b200_eri_get_paths: invalid argument");
+        return CCSD_B200_ERR_ARG;
+    }
+    for (int c = 0; c < 81; c++)
+        choice[c] = (uint8_t)g_paths[deriv].force(c / 27, (c / 9) % 3, (c / 3) % 3, c % 3);
+    return CCSD_B200_OK;
 }
 
 int ccsd_b200_eri_quartet_checksums(int deriv, const int32_t *atm, const int32_t *bas, const double *env,

@@ -199,7 +199,17 @@ __device__ __forceinline__ void build_pair_tables(const Shell &si, const Shell &
 // per thread: Rys node/weight r of pq and the recurrence coefficients,
 // written to par[(s - s0) * kParStride + 0..10].  With tab == nullptr the
 // pair rows are computed here (contractions too long for the table).
-__device__ __forceinline__ void slot_params(const double *__restrict__ tab, const Shell &si, const Shell &sj,
+// Phase A is called once per slot batch; CB_SLOT_NOINLINE = 1 keeps one
+// copy of it for all the kernels' code paths instead of one per path.
+#ifndef CB_SLOT_NOINLINE
+#define CB_SLOT_NOINLINE 0
+#endif
+#if CB_SLOT_NOINLINE
+#define CB_SLOT_INLINE __noinline__
+#else
+#define CB_SLOT_INLINE __forceinline__
+#endif
+__device__ CB_SLOT_INLINE void slot_params(const double *__restrict__ tab, const Shell &si, const Shell &sj,
                                             const Shell &sk, const Shell &sl, const PairMask &mb,
                                             const PairMask &mk, const double *__restrict__ AB, double rab2,
                                             const double *__restrict__ CD, double rcd2, int nroots, double pref0,
@@ -392,6 +402,12 @@ struct S2klOut {
     double *out;
     long long nao_pair, comp_stride;
     int nao, i_base;
+    // spherical s2kl output (c2s set; l <= 2 kernels): cart->sph factors of a
+    // d shell, c2s[s * 6 + c] (s and p: identity), and the spherical AO offset
+    // of every shell; out, nao, nao_pair, comp_stride and i_base then describe
+    // the spherical block
+    const double *c2s;
+    const int *ao_sph;
     // MODE_GRAD: rows [g_row0, g_row0 + g_rows) of the dense [nao]^4 density in
     // the Cartesian AO basis (all rows: g_row0 = 0, g_rows = nao)
     const double *gamma;
@@ -407,20 +423,76 @@ struct S2klOut {
     }
 };
 
+template <int NT>
+__device__ __forceinline__ void grp_sync();
+
+// Spherical s2kl epilogue.  The quartet's Cartesian block, staged in shared
+// memory as a[c][fi][fj][fk][fl] (shells in the quartet's own order, nc
+// components), is transformed one index at a time (l, k, j, i; d shells only,
+// the s and p factors are the identity), alternating between a and b (each
+// nc * nf doubles), and written to the spherical s2kl block (k >= l within a
+// shell pair with ksh == lsh).  bad: the block did not fit the shared-memory
+// staging; its outputs are written as NaN so the failure cannot pass silently.
+template <int NT>
+__device__ void s2kl_sph_store(double *__restrict__ a, double *__restrict__ b, int nc, int li, int lj, int lk,
+                               int ll, int ish, int jsh, int ksh, int lsh, const S2klOut &so, int lane, bool bad)
+{
+    const int L[4] = {li, lj, lk, ll};
+    int n[4] = {ncart(li), ncart(lj), ncart(lk), ncart(ll)};
+    double *src = a, *dst = b;
+    for (int x = 3; x >= 0; x--) {
+        if (L[x] < 2 || bad) continue;
+        int outer = nc, inner = 1;
+        for (int y = 0; y < x; y++) outer *= n[y];
+        for (int y = x + 1; y < 4; y++) inner *= n[y];
+        const int m = 2 * L[x] + 1, nx = n[x];
+        grp_sync<NT>();
+        for (int e = lane; e < outer * m * inner; e += NT) {
+            const int in = e % inner, t = e / inner;
+            const int sidx = t % m, o = t / m;
+            const double *sp = src + o * nx * inner + in;
+            const double *cr = so.c2s + sidx * 6;
+            double v = 0.0;
+            for (int c = 0; c < nx; c++) v = fma(cr[c], sp[c * inner], v);
+            dst[e] = v;
+        }
+        n[x] = m;
+        double *t = src;
+        src = dst;
+        dst = t;
+    }
+    grp_sync<NT>();
+    const int i0 = so.ao_sph[ish] - so.i_base, j0 = so.ao_sph[jsh], k0 = so.ao_sph[ksh], l0 = so.ao_sph[lsh];
+    const int nl = 2 * ll + 1, nk = 2 * lk + 1, nj = 2 * lj + 1, ni = 2 * li + 1;
+    for (int e = lane; e < nc * ni * nj * nk * nl; e += NT) {
+        int t = e;
+        const int fl = t % nl; t /= nl;
+        const int fk = t % nk; t /= nk;
+        const int fj = t % nj; t /= nj;
+        const int fi = t % ni;
+        const int c = t / ni;
+        if (ksh == lsh && fl > fk) continue;
+        const long long k = k0 + fk, l = l0 + fl;
+        so.out[c * so.comp_stride + ((long long)(i0 + fi) * so.nao + (j0 + fj)) * so.nao_pair + k * (k + 1) / 2 + l] =
+            bad ? __longlong_as_double(0x7ff8000000000000ll) : src[e];
+    }
+    grp_sync<NT>();
+}
+
 // Integrals of one shell quartet by one warp.  MODE_S2KL writes the s2kl block,
 // MODE_QSUM writes two checksums per component of the Cartesian quartet block,
 // MODE_GRAD contracts the block with so.gamma: per component
 //   q[c] += w * sum_{ijkl in the block} I_c[ijkl] gamma[ijkl],
 // w = 1 for k shell == l shell (the full k,l block) and 2 otherwise (the
 // (l,k) half of a gamma that is symmetric in k <-> l).
-template <int D, int MODE, bool LOW>
+// GW outputs per lane and chunk (eri_quartet_any sizes it to the block).
+template <int D, int MODE, bool LOW, int GW = 8>
 __device__ void eri_quartet(const int *__restrict__ atm, const int *__restrict__ bas,
                             const double *__restrict__ env, const int *__restrict__ ao_loc,
                             int ish, int jsh, int ksh, int lsh, double *__restrict__ wsm, int smem_warp,
                             const S2klOut &so, double *__restrict__ qsum, int lane)
 {
     constexpr int NC = D ? 3 : 1;
-    constexpr int GW = 8;
     const Shell si = load_shell(atm, bas, env, ish), sj_ = load_shell(atm, bas, env, jsh);
     const Shell sk_ = load_shell(atm, bas, env, ksh), sl_ = load_shell(atm, bas, env, lsh);
     const int li = si.l, lj = sj_.l, lk = sk_.l, ll = sl_.l;
@@ -494,7 +566,7 @@ __device__ void eri_quartet(const int *__restrict__ atm, const int *__restrict__
             for (int it = lane; it < (s1 - s0) * 3; it += 32) {
                 const int s = it / 3, dir = it - s * 3;
                 build_g_any<D, LOW>(par + s * kParStride, dir, li, lj, lk, ll, AB[dir], CD[dir],
-                               gbuf + (s * 3 + dir) * gst);
+                                    gbuf + (s * 3 + dir) * gst);
             }
             __syncwarp();
             // ---- phase C: accumulate
@@ -532,7 +604,23 @@ __device__ void eri_quartet(const int *__restrict__ atm, const int *__restrict__
                     for (int o = FW; o < 32; o <<= 1) acc[n][c] += __shfl_xor_sync(0xffffffffu, acc[n][c], o);
         }
         // ---- epilogue
-        if (MODE == MODE_S2KL) {
+        if (MODE == MODE_S2KL && so.c2s) {
+            // spherical output: the block (one chunk of at most FW * GW
+            // functions on this path) is staged over the dead slot buffers
+            __syncwarp();
+            const bool bad = nf > FW * GW || 2 * NC * nf > smem_warp;
+            double *a = wsm, *b = wsm + NC * nf;
+            if (!bad) {
+#pragma unroll
+                for (int n = 0; n < GW; n++) {
+                    const int f = f0 + n * FW + flane;
+                    if (f < nf && grp == 0)
+#pragma unroll
+                        for (int c = 0; c < NC; c++) a[c * nf + f] = acc[n][c];
+                }
+            }
+            s2kl_sph_store<32>(a, b, NC, li, lj, lk, ll, ish, jsh, ksh, lsh, so, lane, bad);
+        } else if (MODE == MODE_S2KL) {
             const int i0 = ao_loc[ish] - so.i_base, j0 = ao_loc[jsh], k0 = ao_loc[ksh], l0 = ao_loc[lsh];
 #pragma unroll
             for (int n = 0; n < GW; n++) {
@@ -613,6 +701,29 @@ __device__ void eri_quartet(const int *__restrict__ atm, const int *__restrict__
             }
         }
     }
+}
+
+// The per-output path with GW sized to the block: every lane holds at most
+// ceil(nf / FW) outputs (FW lanes per slot group), so the unrolled output
+// loop of the slot accumulation has no iterations that no lane uses; blocks
+// of more than 8 FW functions run in chunks of 8 per lane.
+template <int D, int MODE, bool LOW>
+__device__ __forceinline__ void eri_quartet_any(const int *__restrict__ atm, const int *__restrict__ bas,
+                                                const double *__restrict__ env, const int *__restrict__ ao_loc,
+                                                int ish, int jsh, int ksh, int lsh, double *__restrict__ wsm,
+                                                int smem_warp, const S2klOut &so, double *__restrict__ qsum,
+                                                int lane, int nf)
+{
+    const int fw = nf >= 32 ? 32 : (nf > 16 ? 32 : (nf > 8 ? 16 : (nf > 4 ? 8 : (nf > 2 ? 4 : (nf > 1 ? 2 : 1)))));
+    const int per = (nf + fw - 1) / fw;
+    if (per <= 1)
+        eri_quartet<D, MODE, LOW, 1>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, wsm, smem_warp, so, qsum, lane);
+    else if (per <= 2)
+        eri_quartet<D, MODE, LOW, 2>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, wsm, smem_warp, so, qsum, lane);
+    else if (per <= 4)
+        eri_quartet<D, MODE, LOW, 4>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, wsm, smem_warp, so, qsum, lane);
+    else
+        eri_quartet<D, MODE, LOW, 8>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, wsm, smem_warp, so, qsum, lane);
 }
 
 // ===========================================================================
@@ -791,10 +902,14 @@ struct HcPlan {
 #endif
 static constexpr int kHcMaxG = 8;       // groups per lane on a warp (grouped form)
 
+// force: 0 the measured rule below, 1 this path whenever the quartet fits,
+// 2 never (the per-output path); the warp kernels take it per L-class from
+// the autotuner's table (PathTable).
 __device__ __forceinline__ bool hc_plan(int D, int li, int lj, int lk, int ll, HcPlan &h,
-                                        int maxacc = 32 * kHcMaxJ, int cap = kHcSmem, bool always = false)
+                                        int maxacc = 32 * kHcMaxJ, int cap = kHcSmem, bool always = false,
+                                        int force = 0)
 {
-    if (li > 2 || lj > 2 || lk > 2 || ll > 2) return false;
+    if (li > 2 || lj > 2 || lk > 2 || ll > 2 || force == 2) return false;
     h.kswap = lk < ll;
     h.bswap = D == 0 && li < lj;
     if (h.kswap) { const int t = lk; lk = ll; ll = t; }
@@ -833,7 +948,7 @@ __device__ __forceinline__ bool hc_plan(int D, int li, int lj, int lk, int ll, H
     const int nf = hc_ncart(li) * h.nb * h.ncd;
     const int lo = h.nacc > h.nbra * h.ncd ? h.nacc : h.nbra * h.ncd;
     if (h.nacc > maxacc || lo + h.nket > cap) return false;
-    if (always) return true;
+    if (always || force == 1) return true;
     if (CB_HC_RULE == 2 || (CB_HC_RULE == 1 && D)) return true;
     // measured: worth it when the per-output path would recompute the slots
     // for several 256-output chunks, or when [e|f] is clearly smaller than
@@ -1036,6 +1151,12 @@ __device__ void eri_quartet_hc(const int *__restrict__ atm, const int *__restric
     const int nfi = hc_ncart(li), nfj = h.nb, nfk = h.nc, nfl = h.nd;      // computed orientation
     const int nf = nfi * nfj * h.ncd;
     const int onj = h.bswap ? nfi : nfj, onk = h.kswap ? nfl : nfk, onl = h.kswap ? nfk : nfl;   // original
+    // spherical s2kl output: the block is staged above the bra results
+    // (the [e|f] values and ket rows are dead by now)
+    const int slo = h.nacc > h.nbra * h.ncd ? h.nacc : h.nbra * h.ncd;
+    const bool sph = MODE == MODE_S2KL && so.c2s != nullptr;
+    const bool sbad = sph && slo + 2 * NC * nf > cap;
+    double *sa = wsm + slo, *sb = sa + NC * nf;
     double r1[NC], r2[NC];
 #pragma unroll
     for (int c = 0; c < NC; c++) r1[c] = r2[c] = 0.0;
@@ -1064,7 +1185,12 @@ __device__ void eri_quartet_hc(const int *__restrict__ atm, const int *__restric
         int fk = cd / nfl, fl = cd - fk * nfl;
         if (h.kswap) { const int t = fk; fk = fl; fl = t; }
         const int oi = h.bswap ? fj : fi, oj = h.bswap ? fi : fj;
-        if (MODE == MODE_S2KL) {
+        if (MODE == MODE_S2KL && sph) {
+            const int fr = ((oi * onj + oj) * onk + fk) * onl + fl;
+            if (!sbad)
+#pragma unroll
+                for (int c = 0; c < NC; c++) sa[c * nf + fr] = v[c];
+        } else if (MODE == MODE_S2KL) {
             if (ksh == lsh && fl > fk) continue;
             const int i0 = ao_loc[ish] - so.i_base, j0 = ao_loc[jsh], k0 = ao_loc[ksh], l0 = ao_loc[lsh];
             const long long k = k0 + fk, l = l0 + fl;
@@ -1088,6 +1214,11 @@ __device__ void eri_quartet_hc(const int *__restrict__ atm, const int *__restric
                 r2[c] += v[c] * v[c];
             }
         }
+    }
+    if (sph) {
+        grp_sync<NT>();
+        s2kl_sph_store<NT>(sa, sb, NC, h.bswap ? lj : li, h.bswap ? li : lj, h.kswap ? ll : lk, h.kswap ? lk : ll,
+                           ish, jsh, ksh, lsh, so, lane, sbad);
     }
     if (MODE == MODE_QSUM || MODE == MODE_GRAD) {
         const double wkl = MODE == MODE_GRAD && ksh != lsh ? 2.0 : 1.0;
@@ -1433,34 +1564,44 @@ template <int D, bool LOW>
 __global__ void __launch_bounds__(kWarps * 32, 2) eri_s2kl_kernel(
     const int *__restrict__ atm, const int *__restrict__ bas, const double *__restrict__ env,
     const int *__restrict__ ao_loc, int ish0, int ish1, int nbas, int nao, double *__restrict__ out,
-    int smem_warp)
+    int smem_warp, PathTable paths, const int *__restrict__ ao_sph = nullptr, const double *__restrict__ c2s = nullptr)
 {
     extern __shared__ double smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     double *wsm = smem + warp * smem_warp;
     const long long npairs = (long long)nbas * (nbas + 1) / 2;
     const long long nq = (long long)(ish1 - ish0) * nbas * npairs;
-    S2klOut so;
+    // c2s set (l <= 2 kernels): spherical output, nao spherical AOs
+    const int *oloc = LOW && c2s ? ao_sph : ao_loc;
+    S2klOut so = {};
     so.out = out;
     so.nao = nao;
     so.nao_pair = (long long)nao * (nao + 1) / 2;
-    so.comp_stride = (long long)(ao_loc[ish1] - ao_loc[ish0]) * nao * so.nao_pair;
-    so.i_base = ao_loc[ish0];
+    so.comp_stride = (long long)(oloc[ish1] - oloc[ish0]) * nao * so.nao_pair;
+    so.i_base = oloc[ish0];
+    so.c2s = LOW ? c2s : nullptr;
+    so.ao_sph = ao_sph;
     for (long long q = (long long)blockIdx.x * kWarps + warp; q < nq; q += (long long)gridDim.x * kWarps) {
         const long long ij = q / npairs;
         int ksh, lsh;
         decode_pair(q - ij * npairs, ksh, lsh);
         const int ish = ish0 + (int)(ij / nbas), jsh = (int)(ij % nbas);
-        if (quartet_nf(bas, ish, jsh, ksh, lsh) > heavy_nf(D)) continue;
+        const int nfq = quartet_nf(bas, ish, jsh, ksh, lsh);
+        if (nfq > heavy_nf(D)) continue;
         if (LOW) {
             HcPlan h;
-            if (hc_plan(D, bas[ish * CB_BAS_SLOTS + CB_ANG_OF], bas[jsh * CB_BAS_SLOTS + CB_ANG_OF],
-                        bas[ksh * CB_BAS_SLOTS + CB_ANG_OF], bas[lsh * CB_BAS_SLOTS + CB_ANG_OF], h)) {
+            const int li = bas[ish * CB_BAS_SLOTS + CB_ANG_OF], lj = bas[jsh * CB_BAS_SLOTS + CB_ANG_OF];
+            const int lk = bas[ksh * CB_BAS_SLOTS + CB_ANG_OF], ll = bas[lsh * CB_BAS_SLOTS + CB_ANG_OF];
+            // spherical output stages the whole block: the per-output path
+            // holds at most 256 functions, larger blocks take this path
+            const int force = so.c2s && nfq > 256 ? 1 : paths.force(li, lj, lk, ll);
+            if (hc_plan(D, li, lj, lk, ll, h, 32 * kHcMaxJ, kHcSmem, false, force)) {
                 eri_quartet_hc_any<D, MODE_S2KL>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, h, wsm, so, nullptr, lane);
                 continue;
             }
         }
-        eri_quartet<D, MODE_S2KL, LOW>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, wsm, smem_warp, so, nullptr, lane);
+        eri_quartet_any<D, MODE_S2KL, LOW>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, wsm, smem_warp, so, nullptr, lane,
+                                           nfq);
     }
 }
 
@@ -1473,7 +1614,7 @@ __global__ void __launch_bounds__(warps_of(MODE) * 32, 8 / warps_of(MODE)) eri_q
     const int *__restrict__ atm, const int *__restrict__ bas, const double *__restrict__ env,
     const int4 *__restrict__ quartets, long long nq, double *__restrict__ qsum, int smem_warp,
     const int *__restrict__ ao_loc = nullptr, const double *__restrict__ gamma = nullptr, int nao = 0,
-    double *__restrict__ full = nullptr, int heavy = 0, int grow0 = 0, int grows = 0)
+    double *__restrict__ full = nullptr, int heavy = 0, int grow0 = 0, int grows = 0, PathTable paths = {})
 {
     if (heavy <= 0) heavy = heavy_nf(D);
     extern __shared__ double smem[];
@@ -1496,15 +1637,18 @@ __global__ void __launch_bounds__(warps_of(MODE) * 32, 8 / warps_of(MODE)) eri_q
     for (long long t = t0 + warp; t < t1; t += warps_of(MODE)) {
         const long long q = nq - 1 - t;
         const int4 s = quartets[q];
-        if (quartet_nf(bas, s.x, s.y, s.z, s.w) > heavy) continue;
+        const int nfq = quartet_nf(bas, s.x, s.y, s.z, s.w);
+        if (nfq > heavy) continue;
         double acc[NOUT];
         for (int c = 0; c < NOUT; c++) acc[c] = 0.0;
         HcPlan h;
-        if (LOW && hc_plan(D, bas[s.x * CB_BAS_SLOTS + CB_ANG_OF], bas[s.y * CB_BAS_SLOTS + CB_ANG_OF],
-                           bas[s.z * CB_BAS_SLOTS + CB_ANG_OF], bas[s.w * CB_BAS_SLOTS + CB_ANG_OF], h))
+        const int li = bas[s.x * CB_BAS_SLOTS + CB_ANG_OF], lj = bas[s.y * CB_BAS_SLOTS + CB_ANG_OF];
+        const int lk = bas[s.z * CB_BAS_SLOTS + CB_ANG_OF], ll = bas[s.w * CB_BAS_SLOTS + CB_ANG_OF];
+        if (LOW && hc_plan(D, li, lj, lk, ll, h, 32 * kHcMaxJ, kHcSmem, false, paths.force(li, lj, lk, ll)))
             eri_quartet_hc_any<D, MODE>(atm, bas, env, ao_loc, s.x, s.y, s.z, s.w, h, wsm, so, acc, lane);
         else
-            eri_quartet<D, MODE, LOW>(atm, bas, env, ao_loc, s.x, s.y, s.z, s.w, wsm, smem_warp, so, acc, lane);
+            eri_quartet_any<D, MODE, LOW>(atm, bas, env, ao_loc, s.x, s.y, s.z, s.w, wsm, smem_warp, so, acc, lane,
+                                          nfq);
         if (lane == 0)
             for (int c = 0; c < NOUT; c++)
                 if (MODE != MODE_FULL) qsum[q * NOUT + c] = acc[c];
@@ -1516,23 +1660,32 @@ template <int D, bool LOW>
 __global__ void __launch_bounds__(kHeavyThreads, 1) eri_s2kl_heavy_kernel(
     const int *__restrict__ atm, const int *__restrict__ bas, const double *__restrict__ env,
     const int *__restrict__ ao_loc, int ish0, int ish1, int nao, const int4 *__restrict__ quartets, long long nq,
-    double *__restrict__ out, int smem_doubles)
+    double *__restrict__ out, int smem_doubles, const int *__restrict__ ao_sph = nullptr,
+    const double *__restrict__ c2s = nullptr)
 {
     extern __shared__ double smem[];
-    S2klOut so;
+    const int *oloc = LOW && c2s ? ao_sph : ao_loc;
+    S2klOut so = {};
     so.out = out;
     so.nao = nao;
     so.nao_pair = (long long)nao * (nao + 1) / 2;
-    so.comp_stride = (long long)(ao_loc[ish1] - ao_loc[ish0]) * nao * so.nao_pair;
-    so.i_base = ao_loc[ish0];
+    so.comp_stride = (long long)(oloc[ish1] - oloc[ish0]) * nao * so.nao_pair;
+    so.i_base = oloc[ish0];
+    so.c2s = LOW ? c2s : nullptr;
+    so.ao_sph = ao_sph;
     for (long long q = blockIdx.x; q < nq; q += gridDim.x) {
         const int4 s = quartets[q];
         HcPlan h;
-        if (LOW && hc_plan(D, bas[s.x * CB_BAS_SLOTS + CB_ANG_OF], bas[s.y * CB_BAS_SLOTS + CB_ANG_OF],
-                           bas[s.z * CB_BAS_SLOTS + CB_ANG_OF], bas[s.w * CB_BAS_SLOTS + CB_ANG_OF], h,
-                           256 * kHcCtaMaxJ, smem_doubles, true)) {
+        const int li = bas[s.x * CB_BAS_SLOTS + CB_ANG_OF], lj = bas[s.y * CB_BAS_SLOTS + CB_ANG_OF];
+        const int lk = bas[s.z * CB_BAS_SLOTS + CB_ANG_OF], ll = bas[s.w * CB_BAS_SLOTS + CB_ANG_OF];
+        if (LOW && hc_plan(D, li, lj, lk, ll, h, 256 * kHcCtaMaxJ, smem_doubles, true)) {
             eri_quartet_hc_cta<D, MODE_S2KL>(atm, bas, env, ao_loc, s.x, s.y, s.z, s.w, h, smem, smem_doubles, so,
                                              nullptr);
+            continue;
+        }
+        if (so.c2s) {   // spherical output needs the contracted-HRR path: mark the block
+            s2kl_sph_store<kHeavyThreads>(smem, smem, D ? 3 : 1, li, lj, lk, ll, s.x, s.y, s.z, s.w, so, threadIdx.x,
+                                          true);
             continue;
         }
         eri_quartet_cta<D, MODE_S2KL, LOW>(atm, bas, env, ao_loc, s.x, s.y, s.z, s.w, smem, smem_doubles, so, nullptr);
@@ -1594,7 +1747,8 @@ int launch_s2kl(const EriArgs &a, long long grid, size_t smem, cudaStream_t st)
     int rc;
     if ((rc = prepare_kernel(eri_s2kl_kernel<D, LOW>, smem))) return rc;
     eri_s2kl_kernel<D, LOW><<<(int)grid, kWarps * 32, smem, st>>>(a.atm, a.bas, a.env, a.ao_loc, a.ish0, a.ish1,
-                                                                  a.nbas, a.nao, a.out, a.smem_warp);
+                                                                  a.nbas, a.nao, a.out, a.smem_warp,
+                                                                  a.paths, a.ao_sph, a.c2s);
     return check_launch("eri_s2kl_kernel");
 }
 
@@ -1605,7 +1759,7 @@ int launch_s2kl_heavy(const EriArgs &a, long long grid, size_t smem, cudaStream_
     if ((rc = prepare_kernel(eri_s2kl_heavy_kernel<D, LOW>, smem))) return rc;
     eri_s2kl_heavy_kernel<D, LOW><<<(int)grid, kHeavyThreads, smem, st>>>(a.atm, a.bas, a.env, a.ao_loc, a.ish0,
                                                                           a.ish1, a.nao, a.quartets, a.nq, a.out,
-                                                                          a.smem_heavy);
+                                                                          a.smem_heavy, a.ao_sph, a.c2s);
     return check_launch("eri_s2kl_heavy_kernel");
 }
 
@@ -1616,7 +1770,8 @@ int launch_list(const EriArgs &a, long long grid, size_t smem, cudaStream_t st)
     if ((rc = prepare_kernel(eri_qsum_kernel<D, LOW, MODE>, smem))) return rc;
     eri_qsum_kernel<D, LOW, MODE><<<(int)grid, warps_of(MODE) * 32, smem, st>>>(a.atm, a.bas, a.env, a.quartets, a.nq,
                                                                         a.qsum, a.smem_warp, a.ao_loc, a.gamma,
-                                                                        a.nao, a.full, a.heavy, a.grow0, a.grows);
+                                                                        a.nao, a.full, a.heavy, a.grow0, a.grows,
+                                                                        a.paths);
     return check_launch("eri_qsum_kernel");
 }
 

@@ -31,6 +31,25 @@ enum { MODE_S2KL = 0, MODE_QSUM = 1, MODE_GRAD = 2, MODE_FULL = 3 };
 // blocks keep 4-warp CTAs, two per SM (the checksum list ran 19% slower with 8).
 __host__ __device__ constexpr int warps_of(int mode) { return mode == MODE_GRAD || mode == MODE_FULL ? 8 : kWarps; }
 
+// Per-L-class choice of the warp kernels' accumulation path, over the 81
+// classes (li, lj, lk, ll), l <= 2, in the quartet's own shell order, class
+// id li*27 + lj*9 + lk*3 + ll: bit set in hc = contracted-HRR path whenever
+// it fits, bit set in po = per-output path; neither = the measured rule.
+// Passed to the kernels by value (kernel parameter space).
+struct PathTable {
+    unsigned long long hc[2] = {0ull, 0ull}, po[2] = {0ull, 0ull};
+
+    __host__ __device__ int force(int li, int lj, int lk, int ll) const
+    {
+        if (li > 2 || lj > 2 || lk > 2 || ll > 2) return 0;
+        const int c = li * 27 + lj * 9 + lk * 3 + ll;
+        const unsigned long long bit = 1ull << (c & 63);
+        if (hc[c >> 6] & bit) return 1;
+        if (po[c >> 6] & bit) return 2;
+        return 0;
+    }
+};
+
 struct EriArgs {
     const int *atm = nullptr, *bas = nullptr;
     const double *env = nullptr;
@@ -45,6 +64,9 @@ struct EriArgs {
     double *full = nullptr;                        // MODE_FULL dense tensor
     int heavy = 0;                                 // heavy-quartet threshold (0: compiled default)
     int smem_warp = 0, smem_heavy = 0;             // doubles of shared memory per warp / per heavy CTA
+    PathTable paths;                               // accumulation path per L-class (warp kernels)
+    const int *ao_sph = nullptr;                   // s2kl, spherical output: AO offsets per shell
+    const double *c2s = nullptr;                   //   and the d-shell cart->sph factors (5 x 6)
 };
 
 template <int D, bool LOW> int launch_s2kl(const EriArgs &a, long long grid, size_t smem, cudaStream_t st);

@@ -10,6 +10,10 @@ from .basis import _check_mol, get_basis_cached, upload_geometry
 # int2e_ip1 (the same thresholds as heavy_nf() in csrc/eri.cu)
 HEAVY_NF = {0: 1000, 1: 500}
 
+# spherical blocks of l <= 2 bases in one pass (ccsd_b200_eri_s2kl_sph);
+# False: Cartesian kernel + separate sparse transform (the l > 2 route)
+FUSED_SPH = True
+
 
 def heavy_quartets(topo, d0, d1, deriv=0):
     """(n, 4) int32 device list of the block's quartets with more than HEAVY_NF[deriv] functions."""
@@ -49,8 +53,21 @@ def compute_s2kl(mol, b0, b1, deriv, stream=None):
     npc = naoc * (naoc + 1) // 2
     ncomp = 3 if deriv else 1
     st = _native.stream(stream)
-    cart = torch.empty((ncomp, nfc, naoc, npc), dtype=torch.float64, device=dev)
     hq = heavy_quartets(topo, d0, d1, int(deriv))
+    if not mol.cart and topo.lmax <= 2 and FUSED_SPH:
+        # one pass: each quartet's block is transformed to spherical
+        # functions in the kernel that computes it
+        ls_dev, c2s = topo.sph_fused()
+        ls = topo.sph()["ao_loc_sph"]
+        nfs = int(ls[b1] - ls[b0])
+        naos = int(ls[-1])
+        out = torch.empty((ncomp, nfs, naos, naos * (naos + 1) // 2), dtype=torch.float64, device=dev)
+        _native.call("ccsd_b200_eri_s2kl_sph", int(deriv), _native.ptr(atm), _native.ptr(topo.bas_dev),
+                     _native.ptr(env), topo.dc_nbas, _native.ptr(topo.ao_loc_dev), _native.ptr(ls_dev),
+                     _native.ptr(c2s), d0, d1, naos, topo.lmax, _native.ptr(hq), int(hq.shape[0]), _native.ptr(out),
+                     st)
+        return out
+    cart = torch.empty((ncomp, nfc, naoc, npc), dtype=torch.float64, device=dev)
     _native.call("ccsd_b200_eri_s2kl_cart", int(deriv), _native.ptr(atm), _native.ptr(topo.bas_dev),
                  _native.ptr(env), topo.dc_nbas, _native.ptr(topo.ao_loc_dev), d0, d1, naoc, topo.lmax,
                  _native.ptr(hq), int(hq.shape[0]), _native.ptr(cart), st)

@@ -64,6 +64,7 @@ class BasisTopology:
         self.bas_dev = torch.from_numpy(self.dc_bas).to(device)
         self.ao_loc_dev = torch.from_numpy(self.dc_ao_loc).to(device)
         self._sph = None
+        self._sph_fused = None
         self._mol_bas = np.asarray(mol._bas).copy()
         self._sph_src = mol
 
@@ -80,6 +81,28 @@ class BasisTopology:
                              ao_loc_cart=np.asarray(self._sph_src.ao_loc_nr(cart=True)))
             self._sph_src = None
         return self._sph
+
+    def sph_fused(self):
+        """(spherical AO offsets of the decontracted shells, d-shell cart->sph
+        factors 5 x 6) on the device, for ccsd_b200_eri_s2kl_sph (l <= 2)."""
+        if getattr(self, "_sph_fused", None) is None:
+            s = self.sph()
+            C = s["C"]
+            l = self.dc_bas[:, ANG_OF].astype(np.int64)
+            ls = np.zeros(len(l) + 1, dtype=np.int32)
+            np.cumsum(2 * l + 1, out=ls[1:])
+            c2s = np.zeros((5, 6))
+            for d in range(len(l)):
+                lc0, ls0, nc, ns = int(self.dc_ao_loc[d]), int(ls[d]), int((l[d] + 1) * (l[d] + 2) // 2), int(2 * l[d] + 1)
+                blk = C[lc0:lc0 + nc, ls0:ls0 + ns]
+                if l[d] < 2:
+                    if not np.array_equal(blk, np.eye(nc)):
+                        raise ValueError("cart2sph factors of an s or p shell are not the identity")
+                elif l[d] == 2:
+                    c2s = blk.T.copy()
+            self._sph_fused = (torch.from_numpy(ls).to(self.device),
+                               torch.from_numpy(np.ascontiguousarray(c2s)).to(self.device))
+        return self._sph_fused
 
     def sph_block(self, b0, b1):
         """Sparse factors restricted to the i-shell block [b0, b1) (original shells)."""

@@ -91,6 +91,7 @@ def contract_int2e_ip1(mol, gamma, stream=None):
     if nq:
         ds = SimpleNamespace(atm=atm, bas=topo.bas_dev, env=env, lmax=topo.lmax)
         tune.tune_eri_heavy(ds, topo.dc_bas, q, 1, tune.basis_dshare(topo.dc_bas))
+        tune.tune_eri_paths(ds, topo.dc_bas, q, 1, tune.basis_dshare(topo.dc_bas))
     qwork = torch.empty((max(nq, 1), 3), dtype=torch.float64, device=dev)
     out = torch.empty((mol.natm, 3), dtype=torch.float64, device=dev)
     _native.call("ccsd_b200_eri_ip1_contract", _native.ptr(atm), _native.ptr(topo.bas_dev), _native.ptr(env),
@@ -138,6 +139,7 @@ def contract_int2e_ip1_rows(mol, rows, atom, stream=None):
     if nq:
         ds = SimpleNamespace(atm=atm, bas=topo.bas_dev, env=env, lmax=topo.lmax)
         tune.tune_eri_heavy(ds, topo.dc_bas, q, 1, tune.basis_dshare(topo.dc_bas))
+        tune.tune_eri_paths(ds, topo.dc_bas, q, 1, tune.basis_dshare(topo.dc_bas))
     qwork = torch.empty((max(nq, 1), 3), dtype=torch.float64, device=dev)
     seg1 = torch.tensor([0, nq], dtype=torch.int64, device=dev)
     _native.call("ccsd_b200_eri_ip1_contract_rows", _native.ptr(atm), _native.ptr(topo.bas_dev), _native.ptr(env),

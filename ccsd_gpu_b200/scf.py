@@ -49,8 +49,9 @@ def full_eri_gpu(mol):
     atm, env = upload_geometry(mol, dev)
     q = unique_quartets(topo)
     n = topo.nao_cart
-    tune.tune_eri_heavy(SimpleNamespace(atm=atm, bas=topo.bas_dev, env=env, lmax=topo.lmax), topo.dc_bas, q, 0,
-                        tune.basis_dshare(topo.dc_bas))
+    ds = SimpleNamespace(atm=atm, bas=topo.bas_dev, env=env, lmax=topo.lmax)
+    tune.tune_eri_heavy(ds, topo.dc_bas, q, 0, tune.basis_dshare(topo.dc_bas))
+    tune.tune_eri_paths(ds, topo.dc_bas, q, 0, tune.basis_dshare(topo.dc_bas))
     g = torch.empty((n, n, n, n), dtype=torch.float64, device=dev)
     _native.call("ccsd_b200_eri_full_cart", _native.ptr(atm), _native.ptr(topo.bas_dev), _native.ptr(env),
                  _native.ptr(topo.ao_loc_dev), n, _native.ptr(q), int(q.shape[0]), topo.lmax, _native.ptr(g),

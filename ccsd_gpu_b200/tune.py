@@ -1,11 +1,14 @@
 """Measured launch-parameter choices (autotuner), cached per shape class.
 
-Two choices are made by timing candidates on the device:
+Three choices are made by timing candidates on the device:
 
 * ERI list kernels: the Cartesian block size above which a shell quartet runs
   on the CTA-cooperative kernel instead of one warp
   (``ccsd_b200_eri_set_heavy_nf``).  Keyed by the derivative order and the
   L-class / primitive-count signature of the quartet list.
+* ERI warp kernels: the accumulation path (contracted HRR or per output)
+  of every L-class of a quartet list (``ccsd_b200_eri_set_paths``), kept
+  only when the whole list gains.
 * Split-precision GEMMs: the split-K factor, keyed by the GEMM shape
   (M, N, K) and the precision mode, i.e. by (nocc, nvir) through the shapes
   of the CCSD contractions.
@@ -17,6 +20,7 @@ file, so later processes start from measured values.  Timing runs only after
 ``enable()``, and never while a CUDA graph is being captured (the held or
 default choice is used there).
 """
+import ctypes
 import json
 import os
 
@@ -26,7 +30,7 @@ import torch
 from . import _native
 
 ERI_HEAVY_DEFAULT = {0: 1000, 1: 500}      # the library's compiled defaults
-ERI_HEAVY_CANDIDATES = {0: (500, 1000, 2000), 1: (250, 500, 1000)}
+ERI_HEAVY_CANDIDATES = {0: (250, 500, 1000, 2000), 1: (100, 160, 250, 500, 1000)}
 SPLIT_CANDIDATES = (1, 2, 4, 8, 16)
 
 _cache = None
@@ -152,6 +156,94 @@ def tune_eri_heavy(ds, bas, quartets, deriv, dshare, sample=1 << 17, candidates=
         _store(key, int(c))
     set_heavy_nf(deriv, int(c))
     return int(c)
+
+
+# ---- ERI accumulation path per L-class ----------------------------------------------
+ERI_PATH_MIN = 512       # quartets of a class in the list below which the class keeps the compiled rule
+
+
+def set_paths(deriv, choice):
+    """Set the warp kernels' accumulation path per L-class (81 entries: 0 the
+    compiled rule, 1 contracted HRR, 2 per output; class li*27+lj*9+lk*3+ll)."""
+    arr = (ctypes.c_uint8 * 81)(*[int(c) for c in choice])
+    rc = _native.load().ccsd_b200_eri_set_paths(int(deriv), arr, 81)
+    if rc != 0:
+        raise _native.NativeError("ccsd_b200_eri_set_paths failed: %s"
+                                  % _native.load().ccsd_b200_last_error().decode(errors="replace"))
+
+
+def get_paths(deriv):
+    arr = (ctypes.c_uint8 * 81)()
+    rc = _native.load().ccsd_b200_eri_get_paths(int(deriv), arr, 81)
+    if rc != 0:
+        raise _native.NativeError("ccsd_b200_eri_get_paths failed")
+    return [int(c) for c in arr]
+
+
+def class_ids(bas_dev, quartets):
+    """L-class id li*27+lj*9+lk*3+ll of each quartet in its own shell order
+    (-1 when a shell has l > 2), on the device."""
+    l = bas_dev[:, 1].long()[quartets.long()]
+    cid = l[:, 0] * 27 + l[:, 1] * 9 + l[:, 2] * 3 + l[:, 3]
+    return torch.where((l <= 2).all(1), cid, torch.full_like(cid, -1))
+
+
+def tune_eri_paths(ds, bas, quartets, deriv, dshare, per_class=1 << 15, timer=None):
+    """Choose and set the accumulation path of every L-class of lists like
+    ``quartets`` (the arguments of :func:`tune_eri_heavy`; run it first, the
+    heavy threshold decides which quartets the warp kernel sees).
+
+    For each class with at least ERI_PATH_MIN quartets whose blocks run on the
+    warp kernel, the checksum entry point is timed on up to ``per_class`` of
+    its quartets with the class forced onto each path, and the faster path is
+    kept.  The whole table is then kept only if the (sampled) list as a whole
+    runs faster with it than with the compiled rule; otherwise the compiled
+    rule stays.  Returns the table in force."""
+    from .cuda.quartets import quartet_checksums
+    key = eri_key(bas, deriv, dshare) + ":paths"
+    c = cache().get(key)
+    if c is None:
+        if not (_eri_tuning or timer) or torch.cuda.is_current_stream_capturing():
+            set_paths(deriv, [0] * 81)
+            return [0] * 81
+        heavy = get_heavy_nf(deriv)
+        cid = class_ids(ds.bas, quartets)
+        ids, counts = torch.unique(cid, return_counts=True)
+        choice = [0] * 81
+        set_paths(deriv, choice)
+        for k, n in zip(ids.tolist(), counts.tolist()):
+            if k < 0 or n < ERI_PATH_MIN:
+                continue
+            ls = (k // 27, (k // 9) % 3, (k // 3) % 3, k % 3)
+            if int(np.prod([(l + 1) * (l + 2) // 2 for l in ls])) > heavy:
+                continue
+            sel = torch.nonzero(cid == k)[:, 0]
+            if len(sel) > per_class:
+                sel = sel[torch.linspace(0, len(sel) - 1, per_class, device=sel.device).long()]
+            qs = quartets[sel].contiguous()
+            out = torch.empty((len(qs), 3 if deriv else 1, 2), dtype=torch.float64, device=quartets.device)
+
+            def run(p, k=k, qs=qs, out=out):
+                trial = list(choice)
+                trial[k] = p
+                set_paths(deriv, trial)
+                quartet_checksums(ds, qs, deriv, out=out)
+            choice[k], _ = pick([1, 2], run, timer=timer)
+        # keep the table only if the list as a whole gains
+        nq = int(quartets.shape[0])
+        idx = torch.unique(torch.linspace(0, nq - 1, min(1 << 17, nq), device=quartets.device).long())
+        qs = quartets[idx].contiguous()
+        out = torch.empty((len(idx), 3 if deriv else 1, 2), dtype=torch.float64, device=quartets.device)
+        tables = {0: [0] * 81, 1: choice}
+
+        def run_all(t):
+            set_paths(deriv, tables[t])
+            quartet_checksums(ds, qs, deriv, out=out)
+        best, _ = pick([0, 1], run_all, timer=timer)
+        c = "".join(str(v) for v in tables[best])
+        _store(key, c)
+    set_paths(deriv, [int(v) for v in c])
+    return [int(v) for v in c]
 
 
 # ---- split-K factor of the split-precision GEMM ------------------------------------

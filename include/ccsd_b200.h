@@ -54,6 +54,26 @@ int ccsd_b200_eri_s2kl_cart(int deriv, const int32_t *atm, const int32_t *bas, c
                             const int32_t *heavy_quartets, long long n_heavy, double *out, void *stream);
 
 /*
+ * s2kl block in the SPHERICAL basis, computed in one pass: each shell
+ * quartet's Cartesian block is transformed to spherical functions in shared
+ * memory by the kernel that computed it, and only the spherical block is
+ * written.  Shells with l <= 2 only (lmax > 2: CCSD_B200_ERR_UNSUPPORTED; use
+ * ccsd_b200_eri_s2kl_cart and ccsd_b200_cart2sph_s2kl).  Arguments as
+ * ccsd_b200_eri_s2kl_cart, plus ao_loc_sph (nbas + 1 spherical AO offsets of
+ * the decontracted shells) and c2s_d (the 5 x 6 cart->sph factors of a d
+ * shell, row s = spherical function, column = Cartesian function; s and p
+ * shells are the identity); nao_sph is the spherical AO count and out is
+ * (ncomp, ao_loc_sph[ish1] - ao_loc_sph[ish0], nao_sph, nao_sph (nao_sph + 1) / 2).
+ * Replaces compute_int2e_gpu / compute_int2e_ip1_gpu's Cartesian kernel plus
+ * the dense nao_cart^2 unpack and cart->sph transform
+ * (ref: ccsd_gpu/cuda/int2e_gpu.py:110-215, ccsd_gpu/cuda/int2e_ip1_gpu.py:223-330).
+ */
+int ccsd_b200_eri_s2kl_sph(int deriv, const int32_t *atm, const int32_t *bas, const double *env, int nbas,
+                           const int32_t *ao_loc, const int32_t *ao_loc_sph, const double *c2s_d, int ish0, int ish1,
+                           int nao_sph, int lmax, const int32_t *heavy_quartets, long long n_heavy, double *out,
+                           void *stream);
+
+/*
  * Integrals of an explicit list of shell quartets (int32 x 4 per quartet,
  * [i, j, k, l]), consumed in-kernel: per quartet and component two checksums
  *   qsum[q][comp][0] = sum_f v_f * (1 + (f mod 8)/8),  qsum[q][comp][1] = sum_f v_f^2
@@ -77,6 +97,19 @@ int ccsd_b200_eri_quartet_checksums(int deriv, const int32_t *atm, const int32_t
  */
 int ccsd_b200_eri_set_heavy_nf(int deriv, int nf);
 int ccsd_b200_eri_get_heavy_nf(int deriv);
+
+/*
+ * Accumulation path of the warp kernels per L-class, for derivative order
+ * deriv (0 or 1): choice[c], c = li*27 + lj*9 + lk*3 + ll over the 81
+ * classes with every l <= 2 in the quartet's own shell order, is 0 for the
+ * compiled rule, 1 for the contracted-HRR path whenever the quartet fits it,
+ * 2 for the per-output path; n must be 81.  Applies to the s2kl block entry
+ * and the list entry points (process-wide, all devices); set by the
+ * autotuner.  The get call writes the current table.  No counterpart in the
+ * reference (one code path per kernel, ref: ccsd_gpu/cuda/int2e_ip1_module.py:273-667).
+ */
+int ccsd_b200_eri_set_paths(int deriv, const uint8_t *choice, int n);
+int ccsd_b200_eri_get_paths(int deriv, uint8_t *choice, int n);
 
 /*
  * Cartesian -> spherical transform of an s2kl block:

@@ -141,3 +141,23 @@ def test_dense_eri_from_unique_quartets_matches_s2kl_and_oracle(cart):
         if atom.startswith("O"):
             k, l = np.tril_indices(n)
             assert block_close(g[:, :, k, l], oracle_eri.s2kl(mol, 0, mol.nbas, 0))
+
+
+@pytest.mark.parametrize("deriv", [0, 1])
+def test_fused_spherical_blocks_equal_the_two_pass_transform(deriv, monkeypatch):
+    """ccsd_b200_eri_s2kl_sph (spherical blocks written by the ERI kernels
+    themselves) equals the Cartesian kernel followed by the separate sparse
+    transform, on blocks with d shells on every centre, heavy (dd|dd)
+    quartets included."""
+    from ccsd_gpu_b200 import compute_int2e_gpu, compute_int2e_ip1_gpu
+    from ccsd_gpu_b200.cuda import _eri
+    from ccsd_gpu_b200.gto import M
+    mol = M(atom="C 0 0 0; O 0 0 1.2; H 0.9 0 -0.5; H -0.9 0 -0.5", basis="cc-pvdz")
+    fn = compute_int2e_ip1_gpu if deriv else compute_int2e_gpu
+    for b0, b1 in [(0, 3), (4, 6), (mol.nbas - 4, mol.nbas)]:
+        fused = _np(fn(mol, b0, b1))
+        monkeypatch.setattr(_eri, "FUSED_SPH", False)
+        two = _np(fn(mol, b0, b1))
+        monkeypatch.setattr(_eri, "FUSED_SPH", True)
+        assert fused.shape == two.shape and not np.isnan(fused).any(), (b0, b1)
+        assert np.abs(fused - two).max() <= 1e-12 * np.abs(two).max(), (b0, b1)

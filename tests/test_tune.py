@@ -53,3 +53,34 @@ def test_native_heavy_threshold_setter():
             tune.set_heavy_nf(2, 100)
     finally:
         tune.set_heavy_nf(1, old)
+
+
+def test_native_path_table_round_trip():
+    old = [tune.get_paths(d) for d in (0, 1)]
+    try:
+        t = [(c * 7) % 3 for c in range(81)]
+        tune.set_paths(1, t)
+        assert tune.get_paths(1) == t
+        assert tune.get_paths(0) == old[0]          # per derivative order
+        with pytest.raises(_native.NativeError):
+            tune.set_paths(1, [3] + [0] * 80)
+        with pytest.raises(_native.NativeError):
+            tune.set_paths(2, [0] * 81)
+        assert tune.get_paths(1) == t               # a refused table changes nothing
+    finally:
+        for d in (0, 1):
+            tune.set_paths(d, old[d])
+
+
+def test_path_tuner_uses_a_held_table_without_timing(monkeypatch):
+    bas = np.array([[0, 0, 3, 1, 0, 0, 0, 0], [0, 2, 2, 1, 0, 0, 0, 0]])
+    monkeypatch.setattr(tune, "_cache", {})
+    key = tune.eri_key(bas, 1, 0.5) + ":paths"
+    held = "".join(str(c % 3) for c in range(81))
+    tune.cache()[key] = held
+    old = tune.get_paths(1)
+    try:
+        got = tune.tune_eri_paths(None, bas, None, 1, 0.5)      # no device work on this path
+        assert "".join(map(str, got)) == held and tune.get_paths(1) == got
+    finally:
+        tune.set_paths(1, old)

@@ -42,6 +42,34 @@ def test_eri_heavy_threshold_tuning_keeps_checksums():
             assert checksums_close(quartet_checksums(ds, qd, d).cpu().numpy(), ref[d], nf), (d, nf_cut)
 
 
+def test_eri_path_table_and_tuning_keep_checksums():
+    # every l <= 2 class forced onto each accumulation path, and the tuned
+    # table, give the checksums of the compiled rule
+    from ccsd_gpu_b200 import tune, workloads
+    from ccsd_gpu_b200.cuda.quartets import DeviceShells, quartet_checksums, schwarz_bounds
+    sh = workloads.eri_bench_shells(4096, seed=0)
+    ds = DeviceShells(sh)
+    q = workloads.sample_quartets(sh, 8192, seed=7, schwarz_fn=lambda p: schwarz_bounds(ds, p))
+    qd = torch.from_numpy(q).cuda()
+    nf = quartet_nf(sh._bas, q)
+    tune.enable(True)
+    for d in (0, 1):
+        old = tune.get_paths(d)
+        try:
+            tune.set_paths(d, [0] * 81)
+            ref = quartet_checksums(ds, qd, d).cpu().numpy()
+            for forced in (1, 2):
+                tune.set_paths(d, [forced] * 81)
+                assert checksums_close(quartet_checksums(ds, qd, d).cpu().numpy(), ref, nf), (d, forced)
+            tune.set_paths(d, [0] * 81)
+            dshare = float((sh._bas[:, 1][q].max(1) >= 2).mean())
+            t = tune.tune_eri_paths(ds, sh._bas, qd, d, dshare, per_class=1024)
+            assert tune.get_paths(d) == t and set(t) <= {0, 1, 2}
+            assert checksums_close(quartet_checksums(ds, qd, d).cpu().numpy(), ref, nf), (d, "tuned")
+        finally:
+            tune.set_paths(d, old)
+
+
 def test_gemm_split_tuning_keeps_the_product():
     from ccsd_gpu_b200 import tune
     from ccsd_gpu_b200.contract import contract
