@@ -130,7 +130,7 @@ static int smem_per_warp(int lmax, int deriv)
 static int heavy_smem_doubles(int lmax, int deriv)
 {
     const int gsz = (lmax + 1 + deriv) * (lmax + 1) * (lmax + 1) * (lmax + 1);
-    const long long want = (long long)kMaxSlots * (3 * (gsz | 1) + kParStride);
+    const long long want = (long long)(lmax <= 2 ? kMaxSlotsCta : kMaxSlots) * (3 * (gsz | 1) + kParStride);
     const long long cap = 200 * 1024 / 8;
     return (int)(want < cap ? want : cap);
 }

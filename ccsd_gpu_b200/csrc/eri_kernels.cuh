@@ -199,17 +199,7 @@ __device__ __forceinline__ void build_pair_tables(const Shell &si, const Shell &
 // per thread: Rys node/weight r of pq and the recurrence coefficients,
 // written to par[(s - s0) * kParStride + 0..10].  With tab == nullptr the
 // pair rows are computed here (contractions too long for the table).
-// Phase A is called once per slot batch; CB_SLOT_NOINLINE = 1 keeps one
-// copy of it for all the kernels' code paths instead of one per path.
-#ifndef CB_SLOT_NOINLINE
-#define CB_SLOT_NOINLINE 0
-#endif
-#if CB_SLOT_NOINLINE
-#define CB_SLOT_INLINE __noinline__
-#else
-#define CB_SLOT_INLINE __forceinline__
-#endif
-__device__ CB_SLOT_INLINE void slot_params(const double *__restrict__ tab, const Shell &si, const Shell &sj,
+__device__ __forceinline__ void slot_params(const double *__restrict__ tab, const Shell &si, const Shell &sj,
                                             const Shell &sk, const Shell &sl, const PairMask &mb,
                                             const PairMask &mk, const double *__restrict__ AB, double rab2,
                                             const double *__restrict__ CD, double rcd2, int nroots, double pref0,
@@ -889,17 +879,6 @@ struct HcPlan {
     bool kswap, bswap;
 };
 
-// Which l <= 2 quartets take the contracted-HRR path on a warp (CB_HC_RULE):
-// 0 the measured rule of hc_plan(), 1 every int2e_ip1 quartet that fits,
-// 2 every quartet that fits.
-#ifndef CB_HC_RULE
-#define CB_HC_RULE 0
-#endif
-// Grouped accumulation on the contracted-HRR path (0: one accumulator per
-// [e|f] value and lane, the form before grouping).
-#ifndef CB_HC_GROUPED
-#define CB_HC_GROUPED 1
-#endif
 static constexpr int kHcMaxG = 8;       // groups per lane on a warp (grouped form)
 
 // force: 0 the measured rule below, 1 this path whenever the quartet fits,
@@ -949,7 +928,6 @@ __device__ __forceinline__ bool hc_plan(int D, int li, int lj, int lk, int ll, H
     const int lo = h.nacc > h.nbra * h.ncd ? h.nacc : h.nbra * h.ncd;
     if (h.nacc > maxacc || lo + h.nket > cap) return false;
     if (always || force == 1) return true;
-    if (CB_HC_RULE == 2 || (CB_HC_RULE == 1 && D)) return true;
     // measured: worth it when the per-output path would recompute the slots
     // for several 256-output chunks, or when [e|f] is clearly smaller than
     // the output block and the ket has no s shell
@@ -1031,7 +1009,7 @@ __device__ void eri_quartet_hc(const int *__restrict__ atm, const int *__restric
     int tabn = (mb.n + mk.n) * kPairStride;
     if (!pair_table_fits(tabn, cap, 3 * s2t + kParStride, nslot)) tabn = 0;
     int ns = (cap - tabn) / (3 * s2t + kParStride);
-    ns = ns > kMaxSlots ? kMaxSlots : ns;
+    ns = ns > (NT > 32 ? kMaxSlotsCta : kMaxSlots) ? (NT > 32 ? kMaxSlotsCta : kMaxSlots) : ns;
     double *tab = tabn ? wsm : nullptr;
     double *par = wsm + tabn;
     double *gbuf = par + ns * kParStride;
@@ -1298,20 +1276,19 @@ __device__ __forceinline__ void eri_quartet_hc_any(const int *__restrict__ atm, 
                                                    double *__restrict__ wsm, const S2klOut &so,
                                                    double *__restrict__ qsum, int lane)
 {
-    if (CB_HC_GROUPED) {
-        const int ng = (h.ngrp + 31) / 32;
-        if (ng <= kHcMaxG) {
-            if (h.ze == 1)
-                eri_quartet_hcg<D, MODE, 32, 1>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, h, wsm, so, qsum, lane,
-                                                kHcSmem, ng);
-            else if (h.ze == 2)
-                eri_quartet_hcg<D, MODE, 32, 2>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, h, wsm, so, qsum, lane,
-                                                kHcSmem, ng);
-            else
-                eri_quartet_hcg<D, MODE, 32, 3>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, h, wsm, so, qsum, lane,
-                                                kHcSmem, ng);
-            return;
-        }
+    // grouped accumulation when the groups fit the lane's registers
+    const int ng = (h.ngrp + 31) / 32;
+    if (ng <= kHcMaxG) {
+        if (h.ze == 1)
+            eri_quartet_hcg<D, MODE, 32, 1>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, h, wsm, so, qsum, lane,
+                                            kHcSmem, ng);
+        else if (h.ze == 2)
+            eri_quartet_hcg<D, MODE, 32, 2>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, h, wsm, so, qsum, lane,
+                                            kHcSmem, ng);
+        else
+            eri_quartet_hcg<D, MODE, 32, 3>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, h, wsm, so, qsum, lane,
+                                            kHcSmem, ng);
+        return;
     }
     const int nj = (h.nacc + 31) / 32;
     if (nj <= 8)
@@ -1337,20 +1314,18 @@ __device__ __forceinline__ void eri_quartet_hc_cta(const int *__restrict__ atm, 
                                                    double *__restrict__ sm, int cap, const S2klOut &so,
                                                    double *__restrict__ qsum)
 {
-    if (CB_HC_GROUPED) {
-        const int ng = (h.ngrp + 255) / 256;
-        if (ng <= 4) {
-            if (h.ze == 1)
-                eri_quartet_hcg<D, MODE, 256, 1>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, h, sm, so, qsum,
-                                                 threadIdx.x, cap, ng);
-            else if (h.ze == 2)
-                eri_quartet_hcg<D, MODE, 256, 2>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, h, sm, so, qsum,
-                                                 threadIdx.x, cap, ng);
-            else
-                eri_quartet_hcg<D, MODE, 256, 3>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, h, sm, so, qsum,
-                                                 threadIdx.x, cap, ng);
-            return;
-        }
+    const int ng = (h.ngrp + 255) / 256;
+    if (ng <= 4) {
+        if (h.ze == 1)
+            eri_quartet_hcg<D, MODE, 256, 1>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, h, sm, so, qsum,
+                                             threadIdx.x, cap, ng);
+        else if (h.ze == 2)
+            eri_quartet_hcg<D, MODE, 256, 2>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, h, sm, so, qsum,
+                                             threadIdx.x, cap, ng);
+        else
+            eri_quartet_hcg<D, MODE, 256, 3>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, h, sm, so, qsum,
+                                             threadIdx.x, cap, ng);
+        return;
     }
     if (h.nacc <= 256 * 8)
         eri_quartet_hc<D, MODE, 8, 256>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, h, sm, so, qsum, threadIdx.x, cap);
@@ -1559,9 +1534,43 @@ __device__ void eri_quartet_cta(const int *__restrict__ atm, const int *__restri
 }
 
 
+// A quartet that an l <= 2 heavy kernel cannot place on the contracted-HRR
+// path (none of the l <= 2 classes at the compiled shared-memory sizes; the
+// per-output CTA path is left out of those kernels to save registers): its
+// outputs are written as NaN so the failure cannot pass silently.
+template <int D, int MODE>
+__device__ void quartet_mark_bad(const int *__restrict__ bas, const int *__restrict__ ao_loc, int ish, int jsh,
+                                 int ksh, int lsh, const S2klOut &so, double *__restrict__ qsum)
+{
+    constexpr int NC = D ? 3 : 1;
+    const double nan = __longlong_as_double(0x7ff8000000000000ll);
+    if (MODE == MODE_QSUM || MODE == MODE_GRAD) {
+        if (threadIdx.x < (MODE == MODE_QSUM ? 2 * NC : NC)) qsum[threadIdx.x] = nan;
+        return;
+    }
+    const int ni = ncart(bas[ish * CB_BAS_SLOTS + CB_ANG_OF]), nj = ncart(bas[jsh * CB_BAS_SLOTS + CB_ANG_OF]);
+    const int nk = ncart(bas[ksh * CB_BAS_SLOTS + CB_ANG_OF]), nl = ncart(bas[lsh * CB_BAS_SLOTS + CB_ANG_OF]);
+    for (int e = threadIdx.x; e < ni * nj * nk * nl; e += blockDim.x) {
+        int t = e;
+        const int fl = t % nl; t /= nl;
+        const int fk = t % nk; t /= nk;
+        const int fj = t % nj;
+        const int fi = t / nj;
+        if (MODE == MODE_FULL) {
+            full_store8(so.out, so.nao, ao_loc[ish] + fi, ao_loc[jsh] + fj, ao_loc[ksh] + fk, ao_loc[lsh] + fl, nan);
+        } else if (MODE == MODE_S2KL) {
+            if (ksh == lsh && fl > fk) continue;
+            const long long k = ao_loc[ksh] + fk, l = ao_loc[lsh] + fl;
+            for (int c = 0; c < NC; c++)
+                so.out[c * so.comp_stride + ((long long)(ao_loc[ish] - so.i_base + fi) * so.nao + (ao_loc[jsh] + fj)) *
+                                                so.nao_pair + k * (k + 1) / 2 + l] = nan;
+        }
+    }
+}
+
 // s2kl block of shells [ish0, ish1) x all j x all k >= l (decontracted shells).
 template <int D, bool LOW>
-__global__ void __launch_bounds__(kWarps * 32, 2) eri_s2kl_kernel(
+__global__ void __launch_bounds__(kWarps * 32, kWarpCtas) eri_s2kl_kernel(
     const int *__restrict__ atm, const int *__restrict__ bas, const double *__restrict__ env,
     const int *__restrict__ ao_loc, int ish0, int ish1, int nbas, int nao, double *__restrict__ out,
     int smem_warp, PathTable paths, const int *__restrict__ ao_sph = nullptr, const double *__restrict__ c2s = nullptr)
@@ -1610,7 +1619,7 @@ __global__ void __launch_bounds__(kWarps * 32, 2) eri_s2kl_kernel(
 // heavy: quartets with more Cartesian functions than this go to the CTA kernel
 // (0: heavy_nf(D)); the CTA kernel of the same list gets the same value.
 template <int D, bool LOW, int MODE = MODE_QSUM>
-__global__ void __launch_bounds__(warps_of(MODE) * 32, 8 / warps_of(MODE)) eri_qsum_kernel(
+__global__ void __launch_bounds__(warps_of(MODE) * 32, kWarpCtas * kWarps / warps_of(MODE)) eri_qsum_kernel(
     const int *__restrict__ atm, const int *__restrict__ bas, const double *__restrict__ env,
     const int4 *__restrict__ quartets, long long nq, double *__restrict__ qsum, int smem_warp,
     const int *__restrict__ ao_loc = nullptr, const double *__restrict__ gamma = nullptr, int nao = 0,
@@ -1688,7 +1697,11 @@ __global__ void __launch_bounds__(kHeavyThreads, 1) eri_s2kl_heavy_kernel(
                                           true);
             continue;
         }
-        eri_quartet_cta<D, MODE_S2KL, LOW>(atm, bas, env, ao_loc, s.x, s.y, s.z, s.w, smem, smem_doubles, so, nullptr);
+        if constexpr (LOW)
+            quartet_mark_bad<D, MODE_S2KL>(bas, ao_loc, s.x, s.y, s.z, s.w, so, nullptr);
+        else
+            eri_quartet_cta<D, MODE_S2KL, LOW>(atm, bas, env, ao_loc, s.x, s.y, s.z, s.w, smem, smem_doubles, so,
+                                               nullptr);
     }
 }
 
@@ -1710,19 +1723,50 @@ __global__ void __launch_bounds__(kHeavyThreads, 1) eri_qsum_heavy_kernel(
     so.nao = nao;
     constexpr int NC = D ? 3 : 1;
     constexpr int NOUT = MODE == MODE_QSUM ? 2 * NC : NC;
-    for (long long q = blockIdx.x; q < nq; q += gridDim.x) {
-        const int4 s = quartets[q];
-        if (quartet_nf(bas, s.x, s.y, s.z, s.w) <= heavy) continue;
-        HcPlan h;
-        if (LOW && hc_plan(D, bas[s.x * CB_BAS_SLOTS + CB_ANG_OF], bas[s.y * CB_BAS_SLOTS + CB_ANG_OF],
-                           bas[s.z * CB_BAS_SLOTS + CB_ANG_OF], bas[s.w * CB_BAS_SLOTS + CB_ANG_OF], h,
-                           256 * kHcCtaMaxJ, smem_doubles, true)) {
-            eri_quartet_hc_cta<D, MODE>(atm, bas, env, ao_loc, s.x, s.y, s.z, s.w, h, smem, smem_doubles, so,
-                                        MODE == MODE_FULL ? nullptr : qsum + q * NOUT);
-            continue;
+    // The CTA's quartets are q = blockIdx.x + k gridDim.x.  They are screened
+    // for heavy ones kHeavyThreads at a time, one per thread, and compacted in
+    // shared memory (list order kept), so finding the heavy quartets costs one
+    // parallel load per kHeavyThreads list entries instead of a serial chain of
+    // dependent loads over every entry.
+    __shared__ int hq[kHeavyThreads];
+    __shared__ int wcnt[kHeavyThreads / 32];
+    const int tid = threadIdx.x, hl = tid & 31, hw = tid >> 5;
+    for (long long base = blockIdx.x; base < nq; base += (long long)gridDim.x * kHeavyThreads) {
+        const long long qt = base + (long long)tid * gridDim.x;
+        bool hv = false;
+        if (qt < nq) {
+            const int4 t = quartets[qt];
+            hv = quartet_nf(bas, t.x, t.y, t.z, t.w) > heavy;
         }
-        eri_quartet_cta<D, MODE, LOW>(atm, bas, env, ao_loc, s.x, s.y, s.z, s.w, smem, smem_doubles, so,
-                                      MODE == MODE_FULL ? nullptr : qsum + q * NOUT);
+        const unsigned m = __ballot_sync(0xffffffffu, hv);
+        if (hl == 0) wcnt[hw] = __popc(m);
+        __syncthreads();
+        int off = 0, nh = 0;
+        for (int w = 0; w < kHeavyThreads / 32; w++) {
+            if (w < hw) off += wcnt[w];
+            nh += wcnt[w];
+        }
+        if (hv) hq[off + __popc(m & ((1u << hl) - 1u))] = tid;
+        __syncthreads();
+        for (int ih = 0; ih < nh; ih++) {
+            const long long q = base + (long long)hq[ih] * gridDim.x;
+            const int4 s = quartets[q];
+            HcPlan h;
+            if (LOW && hc_plan(D, bas[s.x * CB_BAS_SLOTS + CB_ANG_OF], bas[s.y * CB_BAS_SLOTS + CB_ANG_OF],
+                               bas[s.z * CB_BAS_SLOTS + CB_ANG_OF], bas[s.w * CB_BAS_SLOTS + CB_ANG_OF], h,
+                               256 * kHcCtaMaxJ, smem_doubles, true)) {
+                eri_quartet_hc_cta<D, MODE>(atm, bas, env, ao_loc, s.x, s.y, s.z, s.w, h, smem, smem_doubles, so,
+                                            MODE == MODE_FULL ? nullptr : qsum + q * NOUT);
+                continue;
+            }
+            if constexpr (LOW)
+                quartet_mark_bad<D, MODE>(bas, ao_loc, s.x, s.y, s.z, s.w, so,
+                                          MODE == MODE_FULL ? nullptr : qsum + q * NOUT);
+            else
+                eri_quartet_cta<D, MODE, LOW>(atm, bas, env, ao_loc, s.x, s.y, s.z, s.w, smem, smem_doubles, so,
+                                              MODE == MODE_FULL ? nullptr : qsum + q * NOUT);
+        }
+        __syncthreads();    // hq, wcnt are rewritten by the next screening step
     }
 }
 

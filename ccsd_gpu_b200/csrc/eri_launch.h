@@ -8,9 +8,15 @@ namespace cb {
 
 static constexpr int kWarps = 4;          // warps (quartets in flight) per CTA of the warp kernels (default)
 static constexpr int kHeavyThreads = 256; // threads of the CTA (heavy-quartet) kernels
-static constexpr int kMaxSlots = 64;      // slots per batch cap
+static constexpr int kMaxSlots = 64;      // slots per batch cap (warp kernels, per-output CTA path)
+// slots per batch cap of the contracted-HRR path on a 256-thread CTA: one
+// slot per thread in phase A, three (slot, direction) items per thread in B
+// (measured against 64: heavy int2e_ip1 quartets of the benchmark list 11.0
+// -> 10.75 ms, int2e 3.76 -> 3.56 ms)
+static constexpr int kMaxSlotsCta = 256;
 static constexpr int kParStride = 13;     // doubles of per-slot parameters (odd: lanes spread over banks)
-static constexpr int kHcSmem = 3072;      // doubles of shared memory per warp on the contracted-HRR path
+static constexpr int kHcSmem = 3072;      // doubles of shared memory per warp on the l <= 2 kernels
+static constexpr int kWarpCtas = 2;       // 4-warp CTAs resident per SM (255 registers, kHcSmem doubles per warp)
 
 // Quartets whose Cartesian block has more functions than heavy_nf(D) go to
 // the CTA-cooperative kernel; smaller ones are one warp each.  Measured on the
