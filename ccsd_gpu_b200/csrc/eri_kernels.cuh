@@ -594,7 +594,7 @@ __device__ void eri_quartet(const int *__restrict__ atm, const int *__restrict__
                     for (int o = FW; o < 32; o <<= 1) acc[n][c] += __shfl_xor_sync(0xffffffffu, acc[n][c], o);
         }
         // ---- epilogue
-        if (MODE == MODE_S2KL && so.c2s) {
+        if (MODE == MODE_S2KL_SPH) {
             // spherical output: the block (one chunk of at most FW * GW
             // functions on this path) is staged over the dead slot buffers
             __syncwarp();
@@ -1132,7 +1132,7 @@ __device__ void eri_quartet_hc(const int *__restrict__ atm, const int *__restric
     // spherical s2kl output: the block is staged above the bra results
     // (the [e|f] values and ket rows are dead by now)
     const int slo = h.nacc > h.nbra * h.ncd ? h.nacc : h.nbra * h.ncd;
-    const bool sph = MODE == MODE_S2KL && so.c2s != nullptr;
+    const bool sph = MODE == MODE_S2KL_SPH;
     const bool sbad = sph && slo + 2 * NC * nf > cap;
     double *sa = wsm + slo, *sb = sa + NC * nf;
     double r1[NC], r2[NC];
@@ -1163,7 +1163,7 @@ __device__ void eri_quartet_hc(const int *__restrict__ atm, const int *__restric
         int fk = cd / nfl, fl = cd - fk * nfl;
         if (h.kswap) { const int t = fk; fk = fl; fl = t; }
         const int oi = h.bswap ? fj : fi, oj = h.bswap ? fi : fj;
-        if (MODE == MODE_S2KL && sph) {
+        if (MODE == MODE_S2KL_SPH) {
             const int fr = ((oi * onj + oj) * onk + fk) * onl + fl;
             if (!sbad)
 #pragma unroll
@@ -1569,7 +1569,7 @@ __device__ void quartet_mark_bad(const int *__restrict__ bas, const int *__restr
 }
 
 // s2kl block of shells [ish0, ish1) x all j x all k >= l (decontracted shells).
-template <int D, bool LOW>
+template <int D, bool LOW, bool SPH = false>
 __global__ void __launch_bounds__(kWarps * 32, kWarpCtas) eri_s2kl_kernel(
     const int *__restrict__ atm, const int *__restrict__ bas, const double *__restrict__ env,
     const int *__restrict__ ao_loc, int ish0, int ish1, int nbas, int nao, double *__restrict__ out,
@@ -1580,15 +1580,16 @@ __global__ void __launch_bounds__(kWarps * 32, kWarpCtas) eri_s2kl_kernel(
     double *wsm = smem + warp * smem_warp;
     const long long npairs = (long long)nbas * (nbas + 1) / 2;
     const long long nq = (long long)(ish1 - ish0) * nbas * npairs;
-    // c2s set (l <= 2 kernels): spherical output, nao spherical AOs
-    const int *oloc = LOW && c2s ? ao_sph : ao_loc;
+    // SPH (l <= 2 kernels): spherical output, nao spherical AOs
+    constexpr int M = SPH ? MODE_S2KL_SPH : MODE_S2KL;
+    const int *oloc = SPH ? ao_sph : ao_loc;
     S2klOut so = {};
     so.out = out;
     so.nao = nao;
     so.nao_pair = (long long)nao * (nao + 1) / 2;
     so.comp_stride = (long long)(oloc[ish1] - oloc[ish0]) * nao * so.nao_pair;
     so.i_base = oloc[ish0];
-    so.c2s = LOW ? c2s : nullptr;
+    so.c2s = SPH ? c2s : nullptr;
     so.ao_sph = ao_sph;
     for (long long q = (long long)blockIdx.x * kWarps + warp; q < nq; q += (long long)gridDim.x * kWarps) {
         const long long ij = q / npairs;
@@ -1603,13 +1604,13 @@ __global__ void __launch_bounds__(kWarps * 32, kWarpCtas) eri_s2kl_kernel(
             const int lk = bas[ksh * CB_BAS_SLOTS + CB_ANG_OF], ll = bas[lsh * CB_BAS_SLOTS + CB_ANG_OF];
             // spherical output stages the whole block: the per-output path
             // holds at most 256 functions, larger blocks take this path
-            const int force = so.c2s && nfq > 256 ? 1 : paths.force(li, lj, lk, ll);
+            const int force = SPH && nfq > 256 ? 1 : paths.force(li, lj, lk, ll);
             if (hc_plan(D, li, lj, lk, ll, h, 32 * kHcMaxJ, kHcSmem, false, force)) {
-                eri_quartet_hc_any<D, MODE_S2KL>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, h, wsm, so, nullptr, lane);
+                eri_quartet_hc_any<D, M>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, h, wsm, so, nullptr, lane);
                 continue;
             }
         }
-        eri_quartet_any<D, MODE_S2KL, LOW>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, wsm, smem_warp, so, nullptr, lane,
+        eri_quartet_any<D, M, LOW>(atm, bas, env, ao_loc, ish, jsh, ksh, lsh, wsm, smem_warp, so, nullptr, lane,
                                            nfq);
     }
 }
@@ -1665,7 +1666,7 @@ __global__ void __launch_bounds__(warps_of(MODE) * 32, kWarpCtas * kWarps / warp
 }
 
 // Heavy quartets of the s2kl block (explicit list built by the caller).
-template <int D, bool LOW>
+template <int D, bool LOW, bool SPH = false>
 __global__ void __launch_bounds__(kHeavyThreads, 1) eri_s2kl_heavy_kernel(
     const int *__restrict__ atm, const int *__restrict__ bas, const double *__restrict__ env,
     const int *__restrict__ ao_loc, int ish0, int ish1, int nao, const int4 *__restrict__ quartets, long long nq,
@@ -1673,14 +1674,15 @@ __global__ void __launch_bounds__(kHeavyThreads, 1) eri_s2kl_heavy_kernel(
     const double *__restrict__ c2s = nullptr)
 {
     extern __shared__ double smem[];
-    const int *oloc = LOW && c2s ? ao_sph : ao_loc;
+    constexpr int M = SPH ? MODE_S2KL_SPH : MODE_S2KL;
+    const int *oloc = SPH ? ao_sph : ao_loc;
     S2klOut so = {};
     so.out = out;
     so.nao = nao;
     so.nao_pair = (long long)nao * (nao + 1) / 2;
     so.comp_stride = (long long)(oloc[ish1] - oloc[ish0]) * nao * so.nao_pair;
     so.i_base = oloc[ish0];
-    so.c2s = LOW ? c2s : nullptr;
+    so.c2s = SPH ? c2s : nullptr;
     so.ao_sph = ao_sph;
     for (long long q = blockIdx.x; q < nq; q += gridDim.x) {
         const int4 s = quartets[q];
@@ -1688,11 +1690,11 @@ __global__ void __launch_bounds__(kHeavyThreads, 1) eri_s2kl_heavy_kernel(
         const int li = bas[s.x * CB_BAS_SLOTS + CB_ANG_OF], lj = bas[s.y * CB_BAS_SLOTS + CB_ANG_OF];
         const int lk = bas[s.z * CB_BAS_SLOTS + CB_ANG_OF], ll = bas[s.w * CB_BAS_SLOTS + CB_ANG_OF];
         if (LOW && hc_plan(D, li, lj, lk, ll, h, 256 * kHcCtaMaxJ, smem_doubles, true)) {
-            eri_quartet_hc_cta<D, MODE_S2KL>(atm, bas, env, ao_loc, s.x, s.y, s.z, s.w, h, smem, smem_doubles, so,
+            eri_quartet_hc_cta<D, M>(atm, bas, env, ao_loc, s.x, s.y, s.z, s.w, h, smem, smem_doubles, so,
                                              nullptr);
             continue;
         }
-        if (so.c2s) {   // spherical output needs the contracted-HRR path: mark the block
+        if (SPH) {   // spherical output needs the contracted-HRR path: mark the block
             s2kl_sph_store<kHeavyThreads>(smem, smem, D ? 3 : 1, li, lj, lk, ll, s.x, s.y, s.z, s.w, so, threadIdx.x,
                                           true);
             continue;
@@ -1789,6 +1791,15 @@ template <int D, bool LOW>
 int launch_s2kl(const EriArgs &a, long long grid, size_t smem, cudaStream_t st)
 {
     int rc;
+    if constexpr (LOW) {
+        if (a.c2s) {
+            if ((rc = prepare_kernel(eri_s2kl_kernel<D, LOW, true>, smem))) return rc;
+            eri_s2kl_kernel<D, LOW, true><<<(int)grid, kWarps * 32, smem, st>>>(
+                a.atm, a.bas, a.env, a.ao_loc, a.ish0, a.ish1, a.nbas, a.nao, a.out, a.smem_warp, a.paths, a.ao_sph,
+                a.c2s);
+            return check_launch("eri_s2kl_kernel");
+        }
+    }
     if ((rc = prepare_kernel(eri_s2kl_kernel<D, LOW>, smem))) return rc;
     eri_s2kl_kernel<D, LOW><<<(int)grid, kWarps * 32, smem, st>>>(a.atm, a.bas, a.env, a.ao_loc, a.ish0, a.ish1,
                                                                   a.nbas, a.nao, a.out, a.smem_warp,
@@ -1800,6 +1811,15 @@ template <int D, bool LOW>
 int launch_s2kl_heavy(const EriArgs &a, long long grid, size_t smem, cudaStream_t st)
 {
     int rc;
+    if constexpr (LOW) {
+        if (a.c2s) {
+            if ((rc = prepare_kernel(eri_s2kl_heavy_kernel<D, LOW, true>, smem))) return rc;
+            eri_s2kl_heavy_kernel<D, LOW, true><<<(int)grid, kHeavyThreads, smem, st>>>(
+                a.atm, a.bas, a.env, a.ao_loc, a.ish0, a.ish1, a.nao, a.quartets, a.nq, a.out, a.smem_heavy, a.ao_sph,
+                a.c2s);
+            return check_launch("eri_s2kl_heavy_kernel");
+        }
+    }
     if ((rc = prepare_kernel(eri_s2kl_heavy_kernel<D, LOW>, smem))) return rc;
     eri_s2kl_heavy_kernel<D, LOW><<<(int)grid, kHeavyThreads, smem, st>>>(a.atm, a.bas, a.env, a.ao_loc, a.ish0,
                                                                           a.ish1, a.nao, a.quartets, a.nq, a.out,

@@ -26,7 +26,9 @@ static constexpr int kHeavyNf = 1000;
 static constexpr int kHeavyNfIp1 = 500;
 __host__ __device__ constexpr int heavy_nf(int D) { return D ? kHeavyNfIp1 : kHeavyNf; }
 
-enum { MODE_S2KL = 0, MODE_QSUM = 1, MODE_GRAD = 2, MODE_FULL = 3 };
+// MODE_S2KL_SPH: the s2kl block in spherical functions (l <= 2 kernels), a
+// mode of its own so the Cartesian s2kl kernels carry no staging code
+enum { MODE_S2KL = 0, MODE_QSUM = 1, MODE_GRAD = 2, MODE_FULL = 3, MODE_S2KL_SPH = 4 };
 
 // Warps per CTA of the warp kernel of an epilogue mode.  The molecular lists
 // (the gradient's ip1-Gamma contraction, the SCF's dense ERI tensor) run
