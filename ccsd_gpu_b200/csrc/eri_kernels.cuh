@@ -1641,10 +1641,20 @@ __global__ void __launch_bounds__(warps_of(MODE) * 32, kWarpCtas * kWarps / warp
     // lists are L-class ordered, cheap classes first: walk them from the end
     // so the expensive quartets start first and cheap ones fill the tail.  A
     // block takes one contiguous chunk, so its warps run the same class (and
-    // code path) at the same time.
+    // code path) at the same time; inside the chunk each warp takes the next
+    // quartet from a shared counter, so a warp that drew costly quartets
+    // (many primitives) does not hold the block while the others idle.
     const long long per = (nq + gridDim.x - 1) / gridDim.x;
     const long long t0 = (long long)blockIdx.x * per, t1 = t0 + per < nq ? t0 + per : nq;
-    for (long long t = t0 + warp; t < t1; t += warps_of(MODE)) {
+    __shared__ int next_q;
+    if (threadIdx.x == 0) next_q = 0;
+    __syncthreads();
+    for (;;) {
+        int k = 0;
+        if (lane == 0) k = atomicAdd(&next_q, 1);
+        k = __shfl_sync(0xffffffffu, k, 0);
+        const long long t = t0 + k;
+        if (t >= t1) break;
         const long long q = nq - 1 - t;
         const int4 s = quartets[q];
         const int nfq = quartet_nf(bas, s.x, s.y, s.z, s.w);
