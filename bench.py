@@ -47,10 +47,12 @@ import torch
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# DRAM bytes per ip1 quartet of one step (warp + CTA kernels): dram__bytes
-# rate x duration from an ncu capture of both kernels on an 8192-quartet
-# sample of the benchmark set, (1.742 MB + 0.926 MB) / 8192 quartets
-ERI_DRAM_BYTES_PER_QUARTET = (1.742e6 + 0.926e6) / 8192
+# DRAM bytes per ip1 quartet of one step (warp + CTA kernels):
+# dram__bytes_read.sum + dram__bytes_write.sum of both kernels in one ncu
+# capture on an 8192-quartet sample of the benchmark set (cold caches; the
+# Rys tables and shell data, read once per launch, are included, so the
+# figure scaled to 2^18 quartets is an upper bound): (1.094 MB + 2.297 MB) / 8192
+ERI_DRAM_BYTES_PER_QUARTET = (1.094e6 + 2.297e6) / 8192
 METRIC = "ERI shell quartets/s (FP64 int2e_ip1, 4096 synthetic shells, Schwarz 1e-12); ERI % FP64 peak"
 NSHELL = 4096
 
@@ -965,9 +967,9 @@ def main():
                    "parallelism": "dp%d" % ws if ws > 1 else "single"},
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak, "traffic": ERI_DRAM_BYTES_PER_QUARTET * nq,
-                     "traffic_source": "DRAM bytes of one ncu capture of the ip1 warp and CTA kernels on an "
-                                       "8192-quartet sample of this set, scaled per quartet (shell data is "
-                                       "L2-resident; DRAM traffic grows with the quartet count)",
+                     "traffic_source": "DRAM bytes (read + write) of one ncu capture of the ip1 warp and CTA "
+                                       "kernels on an 8192-quartet sample of this set, scaled per quartet; an "
+                                       "upper bound (per-launch table and shell reads are included)",
                      "peak_source": "FP64 FMA probe measured in this run (driver peaks file has no FP64 figure)",
                      "flops": "reference-algorithm FP64 op count of the primitive quartets of the sample that "
                               "pass the primitive-pair screen (the ones the kernels evaluate)",
