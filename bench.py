@@ -386,7 +386,10 @@ def _lambda_solver(t1, t2, deris, iters, keep):
             l1, l2 = update_lambda_gpu(cc, t1, t2, l1, l2, deris, imds, mode=mode)
         d1 = _gamma1_intermediates_gpu(cc, t1, t2, l1, l2)
         d2 = _gamma2_intermediates_gpu(cc, t1, t2, l1, l2)
-        keep[mode] = (l1, l2, d1, d2)
+        # copies: the compared results must not share storage that a later
+        # solve (of either mode) writes into
+        cp = lambda x: x.clone() if x is not None else None      # noqa: E731
+        keep[mode] = (cp(l1), cp(l2), tuple(cp(x) for x in d1), tuple(cp(x) for x in d2))
     return solve
 
 
